@@ -1,0 +1,181 @@
+/*
+ * opgpu — B200-native multiphase-field time step of OpenPhase, C ABI.
+ *
+ * This is the drop-in boundary for the OpenPhase single-resolution phase-field step.  Every entry
+ * point names the reference interface it replaces (paths relative to the OpenPhase source tree).
+ * Plain C types only: pointers to host memory, sizes and status codes.  No exception ever crosses
+ * this boundary; every call returns OPGPU_OK (0) or a bitmask of OPGPU_E_* codes.
+ *
+ * Threading: one context is driven by one host thread at a time; distinct contexts are
+ * independent.  Each context owns one CUDA stream on its device; calls that return data to the
+ * host are synchronous, opgpu_step returns after the requested steps completed on the device.
+ *
+ * Voxel order everywhere: x slowest, z fastest (v = (x*ny + y)*nz + z), the order of the
+ * reference's Storage3D (include/Containers/Storage3D.h:2054-2064) and of its raw files.
+ */
+#ifndef OPGPU_H
+#define OPGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OPGPU_ABI_VERSION 1
+
+/* ---- codes --------------------------------------------------------------------------------- */
+#define OPGPU_OK                0u
+/* soft conditions raised by the step (the reference would warn or misbehave silently) */
+#define OPGPU_E_OVERFLOW_K      (1u << 0)  /* a voxel ended a step with more than K positive fields */
+#define OPGPU_E_OVERFLOW_LIST   (1u << 1)  /* a voxel's field+candidate list exceeded its capacity   */
+#define OPGPU_E_EMPTY_VOXEL     (1u << 2)  /* finalize left a voxel with no field (reference: UB)     */
+#define OPGPU_E_NORMALIZE_WARN  (1u << 3)  /* NormalizeIncrements plausibility warning                */
+#define OPGPU_E_LIMITER_CAP     (1u << 4)  /* increment limiter stopped after its 25 iterations       */
+#define OPGPU_E_NONFINITE       (1u << 5)  /* a non-finite phase-field value was produced             */
+/* hard errors */
+#define OPGPU_E_INVALID         (1u << 8)  /* invalid argument                                         */
+#define OPGPU_E_CUDA            (1u << 9)  /* CUDA runtime error (message: opgpu_last_error)           */
+#define OPGPU_E_IO              (1u << 10) /* file could not be read or written                         */
+#define OPGPU_E_STATE           (1u << 11) /* call order violated (e.g. step before initialization)     */
+#define OPGPU_E_NODEVICE        (1u << 12) /* no CUDA device / the library was built without one        */
+#define OPGPU_SOFT_MASK         0xFFu
+
+enum opgpu_precision { OPGPU_FP64 = 0, OPGPU_FP32 = 1 };
+enum opgpu_stencil   { OPGPU_STENCIL_SIMPLE = 0, OPGPU_STENCIL_ISOTROPIC = 1, OPGPU_STENCIL_LB = 2 };
+enum opgpu_stage     { OPGPU_STAGE_STABLE = 0, OPGPU_STAGE_SEED = 1, OPGPU_STAGE_NUCLEUS = 2 };
+enum opgpu_pair_mode { OPGPU_PAIRS_PHASE = 0, OPGPU_PAIRS_TABLE = 1, OPGPU_PAIRS_HASH = 2 };
+
+typedef struct opgpu_ctx opgpu_ctx;
+
+/* Grid and storage.  Replaces GridParameters (@GridParameters $Nx,$Ny,$Nz,$dx,$IWidth,
+ * src/GridParameters.cpp:233-265) and the @PhaseField stencil keys (src/PhaseField.cpp:108-178). */
+typedef struct opgpu_grid {
+    int32_t nx, ny, nz;        /* periodic grid                                                   */
+    double  dx;                /* grid spacing                                                    */
+    double  iwidth;            /* interface width in grid cells; Eta = iwidth*dx                  */
+    int32_t laplacian_stencil; /* OPGPU_STENCIL_* ($PhaseFieldLaplacianStencil, default ISOTROPIC) */
+    int32_t gradient_stencil;  /* OPGPU_STENCIL_* ($PhaseFieldGradientStencil, default ISOTROPIC)  */
+    int32_t precision;         /* OPGPU_FP64 (parity drop-in) or OPGPU_FP32                        */
+    int32_t k_slots;           /* stored fields per voxel: 8, 12 or 16                            */
+    int32_t device;            /* CUDA device ordinal                                             */
+} opgpu_grid;
+
+/* Phase-pair model.  Replaces the ISO energy/mobility models of InterfaceProperties
+ * (src/InterfaceProperties.cpp:150-300; InterfaceEnergyModel.h:78-84) and the DrivingForce
+ * limiter settings (src/DrivingForce.cpp:127-168), PhaseField ConsiderNucleusVolume /
+ * NucleusVolumeFactor (src/PhaseField.cpp:112-113). */
+typedef struct opgpu_model {
+    int32_t nphases;               /* <= 8                                                        */
+    const double* sigma;           /* [P*P] interface energy per phase pair ($Sigma_a_b)          */
+    const double* mu;              /* [P*P] interface mobility per phase pair ($Mu_a_b)           */
+    const double* limit;           /* [P*P] driving-force limit ($Limit_a_b) or NULL for 0.95     */
+    int32_t limiting;              /* $Limiting (reference default 1)                             */
+    double  regularization;        /* $RegularizationFactor (default 1.0)                         */
+    double  tj_factor;             /* $TripleJunctionFactor (default 0.0)                         */
+    int32_t consider_nucleus_volume; /* default 1                                                 */
+    double  nucleus_volume_factor;   /* default 1.0                                               */
+} opgpu_model;
+
+typedef struct opgpu_stats {
+    int64_t steps;                 /* steps run since creation                                    */
+    int64_t wide_last;             /* wide-interface voxels (flag != 0) processed by the last step */
+    int64_t wide_total;            /* sum of wide-interface voxels over all steps                 */
+    int64_t entries_in_total;      /* sum over steps of stored entries read                       */
+    int64_t entries_out_total;     /* sum over steps of stored entries written                    */
+    uint32_t status;               /* OR of soft OPGPU_E_* bits since the last opgpu_clear_status  */
+    uint32_t overflow_voxels;      /* voxels that raised OPGPU_E_OVERFLOW_K / _LIST               */
+} opgpu_stats;
+
+/* ---- lifecycle ------------------------------------------------------------------------------ */
+/* Replaces PhaseField::Initialize + AllocateStorages (src/PhaseField.cpp:44-73, 341-365). */
+uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out);
+uint32_t opgpu_destroy(opgpu_ctx* ctx);
+const char* opgpu_last_error(const opgpu_ctx* ctx);
+int32_t  opgpu_abi_version(void);
+/* Number of CUDA devices visible (0 without a GPU). */
+int32_t  opgpu_device_count(void);
+
+/* ---- parameters ----------------------------------------------------------------------------- */
+uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* model);
+/* Grain records: replaces PhaseField::AddGrainInfo (src/PhaseField.cpp:2970-2979) for G grains of
+ * the given phases; stage NULL = all Stable (GrainsProperties.h:319). */
+uint32_t opgpu_set_grains(opgpu_ctx* ctx, int32_t ngrains, const int32_t* phase, const int32_t* stage);
+/* Per-grain-pair interface energy/mobility written into every voxel's interface properties
+ * (what InterfaceProperties::Properties(i,j,k).set_energy_and_mobility would hold after IP.Set,
+ * InterfaceProperties.h:97, NodeIP.h:413-431).  sigma/mu are symmetric [G*G]; either may be NULL
+ * to keep the phase-pair value. */
+uint32_t opgpu_set_pair_table(opgpu_ctx* ctx, const double* sigma, const double* mu);
+/* Per-grain-pair energy generated on the device: sigma(a,b) = lo + span*u(seed, min(a,b), max(a,b))
+ * with the counter-based generator of opgpu_uniform(); for grain counts where a G*G table is
+ * impractical.  Mobility stays the phase-pair value. */
+uint32_t opgpu_set_pair_hash(opgpu_ctx* ctx, uint64_t seed, double lo, double span);
+/* Per-grain driving force dG[G]: on every interface voxel each pair (a before b in the voxel's
+ * list) receives raw = dG[b] - dG[a] (replaces DrivingForce::Clear + NodeDF::add_raw on Force,
+ * src/DrivingForce.cpp:176-183, NodeDF.h:412-435, then Average->SkipAverage :242-274).
+ * NULL disables the driving-force merge. */
+uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG);
+
+/* ---- state ---------------------------------------------------------------------------------- */
+/* Upload ragged per-voxel lists: counts[N], then (idx, val) of all entries concatenated in voxel
+ * order.  Equivalent of PhaseField::Read (src/PhaseField.cpp:2477-2539, NodePF::read
+ * NodePF.h:751-763).  Lists longer than K are accepted if finalize brings them to <= K. */
+uint32_t opgpu_upload_lists(opgpu_ctx* ctx, const int32_t* counts, const int32_t* idx, const double* val);
+/* Read / write a raw PhaseField file (3 x int32 header, per voxel size_t n and n x (size_t index,
+ * double value)); replaces PhaseField::Read(FileName) / Write(FileName)
+ * (src/PhaseField.cpp:2340-2388, 2477-2539). */
+uint32_t opgpu_read_raw(opgpu_ctx* ctx, const char* path);
+uint32_t opgpu_write_raw(opgpu_ctx* ctx, const char* path);
+/* PhaseField::FinalizeInitialization (src/PhaseField.cpp:1068-1077). */
+uint32_t opgpu_finalize_initialization(opgpu_ctx* ctx);
+/* Total stored entries, then download in the opgpu_upload_lists layout. */
+uint32_t opgpu_total_entries(opgpu_ctx* ctx, int64_t* total);
+uint32_t opgpu_download_lists(opgpu_ctx* ctx, int32_t* counts, int32_t* idx, double* val);
+/* Per-voxel flags (0 bulk, 1 interface halo, 2 interface) of the current state
+ * (PhaseField::SetFlagsSR, src/PhaseField.cpp:953-969). */
+uint32_t opgpu_download_flags(opgpu_ctx* ctx, int8_t* flags);
+
+/* ---- the time step -------------------------------------------------------------------------- */
+/* nsteps repetitions of the reference step sequence
+ *   IP.Set -> [dG fill + Average] -> DoubleObstacle::CalculatePhaseFieldIncrements
+ *   (src/DoubleObstacle.cpp:461-571) -> [DrivingForce::MergePhaseFieldIncrements
+ *   (src/DrivingForce.cpp:480-602)] -> PhaseField::NormalizeIncrements (src/PhaseField.cpp:1334-1561)
+ *   -> PhaseField::MergeIncrements + Finalize (src/PhaseField.cpp:1248-1299, 989-1033),
+ * fused into one device pass per step plus a per-grain update.  Returns the soft status bits
+ * raised by these steps (also accumulated in opgpu_stats.status). */
+uint32_t opgpu_step(opgpu_ctx* ctx, double dt, int32_t nsteps);
+/* Same, but does not synchronise: returns once the steps are enqueued on the context's stream.
+ * opgpu_sync waits and returns the accumulated soft status. */
+uint32_t opgpu_step_async(opgpu_ctx* ctx, double dt, int32_t nsteps);
+uint32_t opgpu_sync(opgpu_ctx* ctx);
+/* Grain records after the last step (PhaseField::CalculateGrainsVolume, src/PhaseField.cpp:812-951):
+ * any pointer may be NULL. */
+uint32_t opgpu_grains(opgpu_ctx* ctx, double* volume, double* volume_ratio, double* max_volume,
+                      int32_t* exist, int32_t* stage);
+uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats);
+uint32_t opgpu_clear_status(opgpu_ctx* ctx);
+/* CUDA stream of the context (a cudaStream_t), for callers that order their own work after it. */
+void*    opgpu_stream(opgpu_ctx* ctx);
+
+/* ---- host-side initial states (no GPU needed) ---------------------------------------------- */
+/* Counter-based generator shared by host and device: SplitMix64 (Steele, Lea, Flood 2014) over
+ * the key (seed, stream, a, b); uniform in [0,1) with 53 bits. */
+double   opgpu_uniform(uint64_t seed, uint64_t stream, uint64_t a, uint64_t b);
+/* Voronoi tessellation: G seeds at integer positions floor(u*n) per axis (stream 1, b = axis);
+ * owner[v] = nearest seed under the periodic minimum-image distance, ties to the lowest index.
+ * The reference counterpart is Initializations::VoronoiTessellation (src/Initializations.cpp:
+ * 2014-2194), whose seeds are fixed, so the seeded variant here is what both engines load. */
+uint32_t opgpu_voronoi_owner_host(int32_t nx, int32_t ny, int32_t nz, int32_t ngrains, uint64_t seed,
+                                  int32_t threads, int32_t* owner);
+/* Grain-boundary spreading of an owner map (periodic, order independent): every voxel lists its
+ * own grain first, then each distinct grain among its 26 neighbours in x,y,z-lexicographic offset
+ * order, all with value 1.0 (finalize normalises).  Call with idx == NULL to get counts and the
+ * total; then with idx sized total. */
+uint32_t opgpu_spread_boundaries_host(int32_t nx, int32_t ny, int32_t nz, const int32_t* owner,
+                                      int32_t threads, int32_t* counts, int32_t* idx, int64_t* total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPGPU_H */

@@ -1,0 +1,126 @@
+"""ctypes binding of the opgpu C ABI (include/opgpu.h).
+
+The library is the in-tree build openphase_b200/lib/libopgpu.so.  Loading it needs no GPU; every
+compute entry point reports OPGPU_E_NODEVICE when none is present.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libopgpu.so"
+
+OPGPU_OK = 0
+E_OVERFLOW_K = 1 << 0
+E_OVERFLOW_LIST = 1 << 1
+E_EMPTY_VOXEL = 1 << 2
+E_NORMALIZE_WARN = 1 << 3
+E_LIMITER_CAP = 1 << 4
+E_NONFINITE = 1 << 5
+E_INVALID = 1 << 8
+E_CUDA = 1 << 9
+E_IO = 1 << 10
+E_STATE = 1 << 11
+E_NODEVICE = 1 << 12
+SOFT_MASK = 0xFF
+
+FP64, FP32 = 0, 1
+STENCIL = {"SIMPLE": 0, "ISOTROPIC": 1, "LB": 2}
+STAGE_STABLE, STAGE_SEED, STAGE_NUCLEUS = 0, 1, 2
+
+_CODE_NAMES = {
+    E_OVERFLOW_K: "OVERFLOW_K", E_OVERFLOW_LIST: "OVERFLOW_LIST", E_EMPTY_VOXEL: "EMPTY_VOXEL",
+    E_NORMALIZE_WARN: "NORMALIZE_WARN", E_LIMITER_CAP: "LIMITER_CAP", E_NONFINITE: "NONFINITE",
+    E_INVALID: "INVALID", E_CUDA: "CUDA", E_IO: "IO", E_STATE: "STATE", E_NODEVICE: "NODEVICE",
+}
+
+
+def code_names(code: int):
+    return [n for b, n in _CODE_NAMES.items() if code & b]
+
+
+class OpgpuError(RuntimeError):
+    def __init__(self, code, msg=""):
+        self.code = code
+        super().__init__(f"opgpu error {code:#x} {code_names(code)} {msg}".strip())
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("dx", C.c_double),
+                ("iwidth", C.c_double), ("laplacian_stencil", C.c_int32), ("gradient_stencil", C.c_int32),
+                ("precision", C.c_int32), ("k_slots", C.c_int32), ("device", C.c_int32)]
+
+
+class Model(C.Structure):
+    _fields_ = [("nphases", C.c_int32), ("sigma", C.POINTER(C.c_double)), ("mu", C.POINTER(C.c_double)),
+                ("limit", C.POINTER(C.c_double)), ("limiting", C.c_int32), ("regularization", C.c_double),
+                ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int32),
+                ("nucleus_volume_factor", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("wide_last", C.c_int64), ("wide_total", C.c_int64),
+                ("entries_in_total", C.c_int64), ("entries_out_total", C.c_int64),
+                ("status", C.c_uint32), ("overflow_voxels", C.c_uint32)]
+
+
+_lib = None
+
+# name -> (restype, argtypes); every symbol include/opgpu.h declares
+_P = C.c_void_p
+_SIGS = {
+    "opgpu_create": (C.c_uint32, [C.POINTER(Grid), C.POINTER(_P)]),
+    "opgpu_destroy": (C.c_uint32, [_P]),
+    "opgpu_last_error": (C.c_char_p, [_P]),
+    "opgpu_abi_version": (C.c_int32, []),
+    "opgpu_device_count": (C.c_int32, []),
+    "opgpu_set_model": (C.c_uint32, [_P, C.POINTER(Model)]),
+    "opgpu_set_grains": (C.c_uint32, [_P, C.c_int32, _P, _P]),
+    "opgpu_set_pair_table": (C.c_uint32, [_P, _P, _P]),
+    "opgpu_set_pair_hash": (C.c_uint32, [_P, C.c_uint64, C.c_double, C.c_double]),
+    "opgpu_set_driving_force": (C.c_uint32, [_P, _P]),
+    "opgpu_upload_lists": (C.c_uint32, [_P, _P, _P, _P]),
+    "opgpu_read_raw": (C.c_uint32, [_P, C.c_char_p]),
+    "opgpu_write_raw": (C.c_uint32, [_P, C.c_char_p]),
+    "opgpu_finalize_initialization": (C.c_uint32, [_P]),
+    "opgpu_total_entries": (C.c_uint32, [_P, C.POINTER(C.c_int64)]),
+    "opgpu_download_lists": (C.c_uint32, [_P, _P, _P, _P]),
+    "opgpu_download_flags": (C.c_uint32, [_P, _P]),
+    "opgpu_step": (C.c_uint32, [_P, C.c_double, C.c_int32]),
+    "opgpu_step_async": (C.c_uint32, [_P, C.c_double, C.c_int32]),
+    "opgpu_sync": (C.c_uint32, [_P]),
+    "opgpu_grains": (C.c_uint32, [_P, _P, _P, _P, _P, _P]),
+    "opgpu_get_stats": (C.c_uint32, [_P, C.POINTER(Stats)]),
+    "opgpu_clear_status": (C.c_uint32, [_P]),
+    "opgpu_stream": (_P, [_P]),
+    "opgpu_uniform": (C.c_double, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
+    "opgpu_voronoi_owner_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+                                              C.c_int32, _P]),
+    "opgpu_spread_boundaries_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32, _P, _P,
+                                                  C.POINTER(C.c_int64)]),
+}
+
+
+def lib():
+    """Load libopgpu.so (fails loudly if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise OpgpuError(E_NODEVICE, f"{LIB_PATH} is not built; run python -m openphase_b200.build_ext")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def device_count() -> int:
+    return int(lib().opgpu_device_count())

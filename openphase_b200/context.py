@@ -1,0 +1,163 @@
+"""`Context`: one device-resident phase-field state and its parameters, over the opgpu C ABI."""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import FP32, FP64, STENCIL, Grid, Model, OpgpuError, Stats, lib, ptr
+
+
+def _check(rc: int, h=None, what: str = ""):
+    hard = rc & ~_lib.SOFT_MASK
+    if hard:
+        msg = lib().opgpu_last_error(h).decode() if h else ""
+        raise OpgpuError(rc, f"{what}: {msg}")
+    return rc
+
+
+class Context:
+    """Device state of one simulation (grid, K-slot field storage, grains, parameters)."""
+
+    def __init__(self, nx, ny, nz, *, dx=1.0, iwidth=5.0, stencil="LB", gradient_stencil="ISOTROPIC",
+                 precision="fp64", k_slots=8, device=0):
+        L = lib()
+        g = Grid(nx=nx, ny=ny, nz=nz, dx=dx, iwidth=iwidth, laplacian_stencil=STENCIL[stencil],
+                 gradient_stencil=STENCIL[gradient_stencil], precision=FP32 if precision == "fp32" else FP64,
+                 k_slots=k_slots, device=device)
+        h = C.c_void_p()
+        rc = L.opgpu_create(C.byref(g), C.byref(h))
+        if rc:
+            raise OpgpuError(rc, "opgpu_create")
+        self.h = h
+        self.shape = (nx, ny, nz)
+        self.n = nx * ny * nz
+        self.precision = precision
+        self.k_slots = k_slots
+        self.ngrains = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().opgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- parameters
+    def set_model(self, sigma, mu, *, limit=None, limiting=True, regularization=1.0, tj_factor=0.0,
+                  consider_nucleus_volume=True, nucleus_volume_factor=1.0):
+        sigma = np.ascontiguousarray(np.atleast_2d(sigma), dtype=np.float64)
+        mu = np.ascontiguousarray(np.atleast_2d(mu), dtype=np.float64)
+        lim = None if limit is None else np.ascontiguousarray(np.atleast_2d(limit), dtype=np.float64)
+        m = Model(nphases=sigma.shape[0], sigma=sigma.ctypes.data_as(C.POINTER(C.c_double)),
+                  mu=mu.ctypes.data_as(C.POINTER(C.c_double)),
+                  limit=lim.ctypes.data_as(C.POINTER(C.c_double)) if lim is not None else None,
+                  limiting=int(limiting), regularization=regularization, tj_factor=tj_factor,
+                  consider_nucleus_volume=int(consider_nucleus_volume), nucleus_volume_factor=nucleus_volume_factor)
+        _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
+
+    def set_grains(self, ngrains, phase=None, stage=None):
+        ph = None if phase is None else np.ascontiguousarray(phase, dtype=np.int32)
+        st = None if stage is None else np.ascontiguousarray(stage, dtype=np.int32)
+        _check(lib().opgpu_set_grains(self.h, ngrains, ptr(ph), ptr(st)), self.h, "set_grains")
+        self.ngrains = ngrains
+
+    def set_pair_table(self, sigma=None, mu=None):
+        s = None if sigma is None else np.ascontiguousarray(sigma, dtype=np.float64)
+        m = None if mu is None else np.ascontiguousarray(mu, dtype=np.float64)
+        _check(lib().opgpu_set_pair_table(self.h, ptr(s), ptr(m)), self.h, "set_pair_table")
+
+    def set_pair_hash(self, seed, lo, span):
+        _check(lib().opgpu_set_pair_hash(self.h, seed, lo, span), self.h, "set_pair_hash")
+
+    def set_driving_force(self, dg: Optional[np.ndarray]):
+        d = None if dg is None else np.ascontiguousarray(dg, dtype=np.float64)
+        _check(lib().opgpu_set_driving_force(self.h, ptr(d)), self.h, "set_driving_force")
+
+    # ---- state
+    def upload(self, counts, idx, val):
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        i = np.ascontiguousarray(idx, dtype=np.int32)
+        v = np.ascontiguousarray(val, dtype=np.float64)
+        _check(lib().opgpu_upload_lists(self.h, ptr(c), ptr(i), ptr(v)), self.h, "upload_lists")
+
+    def read_raw(self, path):
+        _check(lib().opgpu_read_raw(self.h, str(path).encode()), self.h, "read_raw")
+
+    def write_raw(self, path):
+        _check(lib().opgpu_write_raw(self.h, str(path).encode()), self.h, "write_raw")
+
+    def finalize_initialization(self) -> int:
+        return _check(lib().opgpu_finalize_initialization(self.h), self.h, "finalize_initialization")
+
+    def step(self, dt, nsteps=1) -> int:
+        return _check(lib().opgpu_step(self.h, dt, nsteps), self.h, "step")
+
+    def step_async(self, dt, nsteps=1):
+        _check(lib().opgpu_step_async(self.h, dt, nsteps), self.h, "step_async")
+
+    def sync(self) -> int:
+        return _check(lib().opgpu_sync(self.h), self.h, "sync")
+
+    def total_entries(self) -> int:
+        t = C.c_int64(0)
+        _check(lib().opgpu_total_entries(self.h, C.byref(t)), self.h, "total_entries")
+        return t.value
+
+    def download(self):
+        total = self.total_entries()
+        counts = np.empty(self.n, dtype=np.int32)
+        idx = np.empty(total, dtype=np.int32)
+        val = np.empty(total, dtype=np.float64)
+        _check(lib().opgpu_download_lists(self.h, ptr(counts), ptr(idx), ptr(val)), self.h, "download_lists")
+        return counts, idx, val
+
+    def flags(self):
+        f = np.empty(self.n, dtype=np.int8)
+        _check(lib().opgpu_download_flags(self.h, ptr(f)), self.h, "download_flags")
+        return f
+
+    def grains(self):
+        G = self.ngrains
+        vol, vr, mx = (np.empty(G) for _ in range(3))
+        ex, st = np.empty(G, dtype=np.int32), np.empty(G, dtype=np.int32)
+        _check(lib().opgpu_grains(self.h, ptr(vol), ptr(vr), ptr(mx), ptr(ex), ptr(st)), self.h, "grains")
+        return {"volume": vol, "volume_ratio": vr, "max_volume": mx, "exist": ex, "stage": st}
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().opgpu_get_stats(self.h, C.byref(s)), self.h, "get_stats")
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def clear_status(self):
+        _check(lib().opgpu_clear_status(self.h), self.h, "clear_status")
+
+    @property
+    def stream(self) -> int:
+        return lib().opgpu_stream(self.h) or 0
+
+    # ---- convenience
+    @classmethod
+    def from_case(cls, case, precision="fp64", k_slots=8, device=0, state=None, threads=0):
+        ctx = cls(case.nx, case.ny, case.nz, dx=case.dx, iwidth=case.iwidth, stencil=case.stencil,
+                  gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
+        ctx.set_model([[case.sigma]], [[case.mu]], limit=[[case.limit]], limiting=case.limiting,
+                      regularization=case.regularization, tj_factor=case.tj_factor)
+        ctx.set_grains(case.ngrains)
+        ps = case.pair_sigma()
+        if ps is not None:
+            ctx.set_pair_table(ps, None)
+        ctx.set_driving_force(case.driving_force())
+        counts, idx, val = state if state is not None else case.initial_state(threads)
+        ctx.upload(counts, idx, val)
+        ctx.finalize_initialization()
+        return ctx

@@ -1,0 +1,781 @@
+// opgpu context: device memory, parameter tables, state upload/download, grain records and the
+// step loop of the C ABI declared in include/opgpu.h.
+#include "opgpu.h"
+#include "opgpu_device.h"
+#include "opgpu_host.h"
+
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace opgpu;
+
+struct opgpu_ctx {
+    opgpu_grid grid{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long n = 0;
+    int K = 8;
+    int fp32 = 0;
+    size_t rsz = 8;
+    // ping-pong state
+    uint8_t* cnt[2] = {nullptr, nullptr};
+    int16_t* idx[2] = {nullptr, nullptr};
+    void* val[2] = {nullptr, nullptr};
+    int cur = 0;
+    // grain records
+    int G = 0;
+    double *d_vr = nullptr, *d_volume = nullptr, *d_maxvol = nullptr, *d_refvol = nullptr, *d_vol_acc = nullptr;
+    int16_t* d_gphase = nullptr;
+    int8_t *d_gstage = nullptr, *d_exist = nullptr;
+    double *d_dg = nullptr, *d_pair_sigma = nullptr, *d_pair_mu = nullptr;
+    uint32_t* d_status = nullptr;
+    unsigned long long* d_counters = nullptr;
+    StepParams sp{};
+    bool model_set = false, state_loaded = false, initialized = false;
+    uint32_t status = 0;
+    double nvf = 1.0;   // NucleusVolumeFactor
+};
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;   // include/Globals.h:124
+
+uint32_t fail(opgpu_ctx* c, uint32_t code, const std::string& msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(ctx, OPGPU_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count)
+{
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T) + 16);
+}
+
+void dfree(void* p)
+{
+    if (p) cudaFree(p);
+}
+
+// ------------------------------------------------------------------------------------ kernels
+
+__device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; }
+
+// Ragged lists -> K-slot state; voxels with more than one entry go through NodePF::finalize
+// (include/Containers/NodePF.h:214-255), which FinalizeSR applies to the flag-2 voxels that
+// NodePF::read produced (NodePF.h:751-763).
+template <class R>
+__global__ void load_kernel(long long N, int K, int G, const int32_t* counts, const long long* offsets,
+                            const int32_t* idx, const double* val, uint8_t* cnt_out, int16_t* idx_out,
+                            R* val_out, uint32_t* status, double* vol_acc)
+{
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const int c = counts[v];
+    const long long off = offsets[v];
+    uint32_t st = 0;
+    if (c > 1)
+    {
+        double total = 0.0;
+        int m = 0;
+        int gs[64];
+        double vs[64];
+        for (int i = 0; i < c; i++)
+        {
+            double w = val[off + i];
+            bool erase = false;
+            if (w >= 1.0 - DBL_EPSILON) w = 1.0;
+            if (w <= 0.0 + DBL_EPSILON) { w = 0.0; erase = true; }
+            total += w;
+            if (!erase && m < 64) { gs[m] = idx[off + i]; vs[m] = w; m++; }
+        }
+        if (m > 1)
+        {
+            const double norm = 1.0 / total;
+            for (int i = 0; i < m; i++) vs[i] *= norm;
+        }
+        else if (m == 1)
+        {
+            vs[0] = 1.0;
+        }
+        else
+        {
+            st |= kStEmptyVoxel;
+        }
+        if (m > K) { st |= kStOverflowK; m = K; }
+        cnt_out[v] = (uint8_t)m;
+        for (int i = 0; i < m; i++)
+        {
+            idx_out[i * N + v] = (int16_t)gs[i];
+            val_out[i * N + v] = (R)vs[i];
+            atomicAdd(&vol_acc[gs[i]], (double)(R)vs[i]);
+        }
+    }
+    else
+    {
+        if (c == 0) st |= kStEmptyVoxel;
+        cnt_out[v] = (uint8_t)c;
+        if (c == 1)
+        {
+            idx_out[v] = (int16_t)idx[off];
+            val_out[v] = (R)val[off];
+            atomicAdd(&vol_acc[idx[off]], (double)(R)val[off]);
+        }
+    }
+    if (st) atomicOr(status, st);
+}
+
+// PhaseField::CalculateGrainsVolume tail (src/PhaseField.cpp:896-951): MAXVolume, VolumeRatio,
+// Exist/Stage bookkeeping; block 0 also rolls the per-step counters into their totals.
+__global__ void grains_update_kernel(int G, double* vol_acc, double* volume, double* maxv, const double* refv,
+                                     double* vr, int8_t* exist, int8_t* stage, unsigned long long* counters,
+                                     int count_step)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g == 0 && count_step)
+    {
+        counters[kCntWideTotal] += counters[kCntWide];
+        counters[kCntEntriesInTotal] += counters[kCntEntriesIn];
+        counters[kCntEntriesOutTotal] += counters[kCntEntriesOut];
+        counters[kCntWideLast] = counters[kCntWide];
+        counters[kCntSteps] += 1;
+        counters[kCntWide] = 0;
+        counters[kCntEntriesIn] = 0;
+        counters[kCntEntriesOut] = 0;
+    }
+    if (g >= G) return;
+    double V = vol_acc[g];
+    vol_acc[g] = 0.0;
+    const double mx = dmax_ref(V, maxv[g]);
+    double r = mx / refv[g];
+    double m = mx;
+    if (exist[g] && V <= 0.0)
+    {
+        exist[g] = 0;
+        stage[g] = OPGPU_STAGE_STABLE;
+        V = 0.0;
+        m = 0.0;
+        r = 1.0;
+    }
+    else if (V > 0.0)
+    {
+        exist[g] = 1;
+        if (stage[g] == OPGPU_STAGE_SEED) stage[g] = OPGPU_STAGE_NUCLEUS;
+        if (r > 1.0)
+        {
+            stage[g] = OPGPU_STAGE_STABLE;
+            r = 1.0;
+        }
+    }
+    volume[g] = V;
+    maxv[g] = m;
+    vr[g] = r;
+}
+
+__global__ void counts_kernel(long long N, const uint8_t* cnt, int32_t* counts, long long* wide)
+{
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < N) { counts[v] = cnt[v]; wide[v] = cnt[v]; }
+}
+
+__global__ void widen_kernel(long long N, const int32_t* counts, long long* wide)
+{
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < N) wide[v] = counts[v];
+}
+
+template <class R>
+__global__ void gather_kernel(long long N, const uint8_t* cnt, const int16_t* idx, const R* val,
+                              const long long* offsets, int32_t* idx_out, double* val_out)
+{
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const int c = cnt[v];
+    const long long off = offsets[v];
+    for (int s = 0; s < c; s++)
+    {
+        idx_out[off + s] = idx[s * N + v];
+        val_out[off + s] = (double)val[s * N + v];
+    }
+}
+
+__global__ void flags_kernel(int nx, int ny, int nz, const uint8_t* cnt, int8_t* flags)
+{
+    const long long N = (long long)nx * ny * nz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const int z = (int)(v % nz);
+    const int y = (int)((v / nz) % ny);
+    const int x = (int)(v / ((long long)ny * nz));
+    int f = cnt[v] > 1 ? 2 : 0;
+    for (int q = 0; q < 27 && f == 0; q++)
+    {
+        const int xx = (x + q / 9 - 1 + nx) % nx, yy = (y + (q / 3) % 3 - 1 + ny) % ny, zz = (z + q % 3 - 1 + nz) % nz;
+        if (cnt[((long long)xx * ny + yy) * nz + zz] > 1) f = 1;
+    }
+    flags[v] = (int8_t)f;
+}
+
+unsigned grid_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+void free_grains(opgpu_ctx* c)
+{
+    dfree(c->d_vr); dfree(c->d_volume); dfree(c->d_maxvol); dfree(c->d_refvol); dfree(c->d_vol_acc);
+    dfree(c->d_gphase); dfree(c->d_gstage); dfree(c->d_exist); dfree(c->d_dg);
+    dfree(c->d_pair_sigma); dfree(c->d_pair_mu);
+    c->d_vr = c->d_volume = c->d_maxvol = c->d_refvol = c->d_vol_acc = nullptr;
+    c->d_gphase = nullptr; c->d_gstage = c->d_exist = nullptr;
+    c->d_dg = c->d_pair_sigma = c->d_pair_mu = nullptr;
+}
+
+// Stencil tables: LaplacianStencil3D_7 / _27a / _LB (include/Containers/LaplacianStencil.h:72-156)
+// and the neighbour sets of GradientStencil1D / 3D / 3D_LB (include/Containers/GradientStencil.h),
+// enumerated in the x, y, z loop order of LaplacianStencil::Set / GradientStencil::Set.
+void set_stencils(StepParams& sp, int lap, int grad, double dx)
+{
+    sp.ns = 0;
+    for (int x = -1; x <= 1; ++x)
+    for (int y = -1; y <= 1; ++y)
+    for (int z = -1; z <= 1; ++z)
+    {
+        const int d = (x != 0) + (y != 0) + (z != 0);
+        double w;
+        if (lap == OPGPU_STENCIL_SIMPLE)
+            w = (d == 0) ? -6.0 : (d == 1 ? 1.0 : 0.0);
+        else if (lap == OPGPU_STENCIL_ISOTROPIC)
+            w = (d == 0) ? -64.0 / 15.0 : (d == 1 ? 7.0 / 15.0 : (d == 2 ? 1.0 / 10.0 : 1.0 / 30.0));
+        else
+            w = (d == 0) ? -38.0 / 9.0 : (d == 1 ? 4.0 / 9.0 : (d == 2 ? 1.0 / 9.0 : 1.0 / 36.0));
+        if (w != 0.0)
+        {
+            sp.lap_d[sp.ns][0] = (signed char)x;
+            sp.lap_d[sp.ns][1] = (signed char)y;
+            sp.lap_d[sp.ns][2] = (signed char)z;
+            sp.lap_w[sp.ns] = w / (dx * dx);
+            sp.ns++;
+        }
+    }
+    // Candidate discovery by the gradient pass only matters when the Laplacian misses neighbours
+    // the gradient stencil visits (SIMPLE Laplacian with a 26-neighbour gradient stencil).
+    sp.ng = 0;
+    if (sp.ns < 27 && grad != OPGPU_STENCIL_SIMPLE)
+    {
+        for (int x = -1; x <= 1; ++x)
+        for (int y = -1; y <= 1; ++y)
+        for (int z = -1; z <= 1; ++z)
+        {
+            if (!x && !y && !z) continue;
+            sp.grad_d[sp.ng][0] = (signed char)x;
+            sp.grad_d[sp.ng][1] = (signed char)y;
+            sp.grad_d[sp.ng][2] = (signed char)z;
+            sp.ng++;
+        }
+    }
+}
+
+uint32_t read_status(opgpu_ctx* ctx)
+{
+    uint32_t st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->status |= st;
+    return st;
+}
+
+uint32_t require(opgpu_ctx* ctx, bool cond, const char* what)
+{
+    if (!ctx) return OPGPU_E_INVALID;
+    if (!cond) return fail(ctx, OPGPU_E_STATE, what);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return fail(ctx, OPGPU_E_CUDA, cudaGetErrorString(e));
+    return OPGPU_OK;
+}
+
+}  // namespace
+
+// ==================================================================================== C ABI
+
+extern "C" int32_t opgpu_abi_version(void) { return OPGPU_ABI_VERSION; }
+
+extern "C" int32_t opgpu_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+extern "C" const char* opgpu_last_error(const opgpu_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
+{
+    if (!grid || !out) return OPGPU_E_INVALID;
+    *out = nullptr;
+    const opgpu_grid& g = *grid;
+    if (g.nx < 3 || g.ny < 3 || g.nz < 3 || !(g.dx > 0.0) || !(g.iwidth > 0.0)) return OPGPU_E_INVALID;
+    if (g.k_slots != 8 && g.k_slots != 12 && g.k_slots != 16) return OPGPU_E_INVALID;
+    if (g.precision != OPGPU_FP64 && g.precision != OPGPU_FP32) return OPGPU_E_INVALID;
+    if (g.laplacian_stencil < 0 || g.laplacian_stencil > 2 || g.gradient_stencil < 0 || g.gradient_stencil > 2)
+        return OPGPU_E_INVALID;
+    if (opgpu_device_count() <= g.device || g.device < 0) return OPGPU_E_NODEVICE;
+    opgpu_ctx* ctx = new opgpu_ctx();
+    ctx->grid = g;
+    ctx->device = g.device;
+    ctx->n = (long long)g.nx * g.ny * g.nz;
+    ctx->K = g.k_slots;
+    ctx->fp32 = g.precision == OPGPU_FP32;
+    ctx->rsz = ctx->fp32 ? sizeof(float) : sizeof(double);
+    auto bail = [&](uint32_t code) { opgpu_destroy(ctx); return code; };
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    for (int b = 0; b < 2; b++)
+    {
+        if (dalloc(&ctx->cnt[b], (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (dalloc(&ctx->idx[b], (size_t)ctx->n * ctx->K) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (cudaMalloc(&ctx->val[b], (size_t)ctx->n * ctx->K * ctx->rsz + 16) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (cudaMemset(ctx->cnt[b], 0, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    }
+    if (dalloc(&ctx->d_status, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    if (dalloc(&ctx->d_counters, kNumCounters) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
+    cudaMemset(ctx->d_counters, 0, kNumCounters * sizeof(unsigned long long));
+    StepParams& sp = ctx->sp;
+    sp.nx = g.nx; sp.ny = g.ny; sp.nz = g.nz; sp.n = ctx->n;
+    set_stencils(sp, g.laplacian_stencil, g.gradient_stencil, g.dx);
+    const double Eta = g.iwidth * g.dx;                 // src/GridParameters.cpp:256
+    sp.pref_do = kPi * kPi / (Eta * Eta);               // src/DoubleObstacle.cpp:504
+    sp.pref_df = kPi / Eta;                             // src/DrivingForce.cpp:507
+    sp.eps_snap = ctx->fp32 ? (double)FLT_EPSILON : DBL_EPSILON;
+    sp.consider_nucleus_volume = 1;
+    sp.limiting = 1;
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(OPGPU_E_CUDA);
+    *out = ctx;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
+{
+    if (!ctx) return OPGPU_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int b = 0; b < 2; b++) { dfree(ctx->cnt[b]); dfree(ctx->idx[b]); dfree(ctx->val[b]); }
+    free_grains(ctx);
+    dfree(ctx->d_status);
+    dfree(ctx->d_counters);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return OPGPU_OK;
+}
+
+extern "C" void* opgpu_stream(opgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    if (!m || m->nphases < 1 || m->nphases > kMaxPhases || !m->sigma || !m->mu)
+        return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: need 1..8 phases and sigma/mu tables");
+    StepParams& sp = ctx->sp;
+    const int P = m->nphases;
+    sp.nphases = P;
+    sp.limiting = m->limiting;
+    sp.tj_factor = m->tj_factor;
+    sp.consider_nucleus_volume = m->consider_nucleus_volume;
+    for (int a = 0; a < P; a++)
+    for (int b = 0; b < P; b++)
+    {
+        const int q = a * P + b;
+        sp.sigma_p[q] = m->sigma[q];
+        sp.mu_p[q] = m->mu[q];
+        const double lim = m->limit ? m->limit[q] : 0.95;   // src/DrivingForce.cpp:161
+        // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor;
+        // the ISO model's MaxEnergy is its Energy (InterfaceEnergyModel.h:82)
+        double allowed = lim * sp.pref_df * m->sigma[q];
+        allowed *= m->regularization;
+        sp.allowed_p[q] = allowed;
+    }
+    ctx->nvf = m->nucleus_volume_factor > 0.0 ? m->nucleus_volume_factor : 1.0;
+    ctx->model_set = true;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_grains(opgpu_ctx* ctx, int32_t ngrains, const int32_t* phase, const int32_t* stage)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->model_set, "opgpu_set_grains: call opgpu_set_model first")) return r;
+    if (ngrains < 1 || ngrains > 32767) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_grains: 1..32767 grains");
+    const int G = ngrains;
+    std::vector<int16_t> gp(G);
+    std::vector<int8_t> gs(G), ex(G, 1);
+    for (int g = 0; g < G; g++)
+    {
+        const int p = phase ? phase[g] : 0;
+        if (p < 0 || p >= ctx->sp.nphases) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_grains: phase out of range");
+        gp[g] = (int16_t)p;
+        const int s = stage ? stage[g] : OPGPU_STAGE_STABLE;
+        if (s < 0 || s > 2) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_grains: bad stage");
+        gs[g] = (int8_t)s;
+    }
+    free_grains(ctx);
+    ctx->G = G;
+    ctx->sp.ngrains = G;
+    CK(dalloc(&ctx->d_vr, G));
+    CK(dalloc(&ctx->d_volume, G));
+    CK(dalloc(&ctx->d_maxvol, G));
+    CK(dalloc(&ctx->d_refvol, G));
+    CK(dalloc(&ctx->d_vol_acc, G));
+    CK(dalloc(&ctx->d_gphase, G));
+    CK(dalloc(&ctx->d_gstage, G));
+    CK(dalloc(&ctx->d_exist, G));
+    // PhaseField::AddGrainInfo (src/PhaseField.cpp:2970-2979): RefVolume from
+    // CalculateReferenceVolume(iWidth) (:367-391, 3-D), VolumeRatio 0, MAXVolume 0, Exist.
+    const double r = ctx->grid.iwidth;
+    const double ref = (4.0 / 3.0) * kPi * r * r * r * ctx->nvf;
+    std::vector<double> refv(G, ref), zeros(G, 0.0);
+    CK(cudaMemcpy(ctx->d_refvol, refv.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_vr, zeros.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_volume, zeros.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_maxvol, zeros.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_vol_acc, zeros.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_gphase, gp.data(), G * sizeof(int16_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_gstage, gs.data(), G * sizeof(int8_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_exist, ex.data(), G * sizeof(int8_t), cudaMemcpyHostToDevice));
+    ctx->sp.pair_mode = OPGPU_PAIRS_PHASE;
+    ctx->sp.use_dg = 0;
+    ctx->initialized = false;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_pair_table(opgpu_ctx* ctx, const double* sigma, const double* mu)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_set_pair_table: call opgpu_set_grains first")) return r;
+    const size_t GG = (size_t)ctx->G * ctx->G;
+    dfree(ctx->d_pair_sigma); ctx->d_pair_sigma = nullptr;
+    dfree(ctx->d_pair_mu); ctx->d_pair_mu = nullptr;
+    if (sigma)
+    {
+        CK(dalloc(&ctx->d_pair_sigma, GG));
+        CK(cudaMemcpy(ctx->d_pair_sigma, sigma, GG * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (mu)
+    {
+        CK(dalloc(&ctx->d_pair_mu, GG));
+        CK(cudaMemcpy(ctx->d_pair_mu, mu, GG * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    ctx->sp.pair_mode = (sigma || mu) ? OPGPU_PAIRS_TABLE : OPGPU_PAIRS_PHASE;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_pair_hash(opgpu_ctx* ctx, uint64_t seed, double lo, double span)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_set_pair_hash: call opgpu_set_grains first")) return r;
+    ctx->sp.pair_mode = OPGPU_PAIRS_HASH;
+    ctx->sp.hash_seed = seed;
+    ctx->sp.hash_lo = lo;
+    ctx->sp.hash_span = span;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_set_driving_force: call opgpu_set_grains first")) return r;
+    if (!dG)
+    {
+        ctx->sp.use_dg = 0;
+        return OPGPU_OK;
+    }
+    if (!ctx->d_dg) CK(dalloc(&ctx->d_dg, ctx->G));
+    CK(cudaMemcpyAsync(ctx->d_dg, dG, ctx->G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->sp.use_dg = 1;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_upload_lists(opgpu_ctx* ctx, const int32_t* counts, const int32_t* idx, const double* val)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_upload_lists: call opgpu_set_grains first")) return r;
+    if (!counts || !idx || !val) return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: null array");
+    const long long N = ctx->n;
+    long long total = 0;
+    for (long long v = 0; v < N; v++)
+    {
+        if (counts[v] < 0 || counts[v] > 64)
+            return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: a voxel list must hold 0..64 entries");
+        total += counts[v];
+    }
+    for (long long q = 0; q < total; q++)
+        if (idx[q] < 0 || idx[q] >= ctx->G) return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: grain index out of range");
+    int32_t *d_counts = nullptr, *d_idx = nullptr;
+    long long *d_off = nullptr, *d_wide = nullptr;
+    double* d_val = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    uint32_t rc = OPGPU_OK;
+    auto cleanup = [&]() { dfree(d_counts); dfree(d_idx); dfree(d_off); dfree(d_wide); dfree(d_val); dfree(d_tmp); };
+    do {
+        cudaError_t e;
+        if ((e = dalloc(&d_counts, N)) != cudaSuccess) break;
+        if ((e = dalloc(&d_off, N)) != cudaSuccess) break;
+        if ((e = dalloc(&d_wide, N)) != cudaSuccess) break;
+        if ((e = dalloc(&d_idx, total)) != cudaSuccess) break;
+        if ((e = dalloc(&d_val, total)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(d_counts, counts, N * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(d_idx, idx, total * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(d_val, val, total * sizeof(double), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) break;
+        widen_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, d_counts, d_wide);
+        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_wide, d_off, N, ctx->stream)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&d_tmp, tmp_bytes + 16)) != cudaSuccess) break;
+        if ((e = cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_wide, d_off, N, ctx->stream)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(ctx->d_vol_acc, 0, ctx->G * sizeof(double), ctx->stream)) != cudaSuccess) break;
+        const int cur = 0;
+        if (ctx->fp32)
+            load_kernel<float><<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->K, ctx->G, d_counts, d_off, d_idx, d_val,
+                ctx->cnt[cur], ctx->idx[cur], static_cast<float*>(ctx->val[cur]), ctx->d_status, ctx->d_vol_acc);
+        else
+            load_kernel<double><<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->K, ctx->G, d_counts, d_off, d_idx, d_val,
+                ctx->cnt[cur], ctx->idx[cur], static_cast<double*>(ctx->val[cur]), ctx->d_status, ctx->d_vol_acc);
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) break;
+        ctx->cur = cur;
+        ctx->state_loaded = true;
+        ctx->initialized = false;
+        e = cudaSuccess;
+        if (e != cudaSuccess) break;
+        cleanup();
+        return OPGPU_OK;
+    } while (0);
+    rc = fail(ctx, OPGPU_E_CUDA, std::string("opgpu_upload_lists: ") + cudaGetErrorString(cudaGetLastError()));
+    cleanup();
+    return rc;
+}
+
+extern "C" uint32_t opgpu_read_raw(opgpu_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return OPGPU_E_INVALID;
+    std::vector<int32_t> counts, idx;
+    std::vector<double> val;
+    std::string err;
+    if (!raw_read(path, ctx->grid.nx, ctx->grid.ny, ctx->grid.nz, counts, idx, val, err))
+        return fail(ctx, OPGPU_E_IO, err);
+    return opgpu_upload_lists(ctx, counts.data(), idx.data(), val.data());
+}
+
+extern "C" uint32_t opgpu_finalize_initialization(opgpu_ctx* ctx)
+{
+    // The upload already applied NodePF::finalize to every multi-entry voxel and accumulated the
+    // grain volumes; what remains of FinalizeSR is the grain-record update.  Flags and candidate
+    // derivatives are re-derived by every step.
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded, "opgpu_finalize_initialization: no state uploaded")) return r;
+    if (ctx->initialized) return fail(ctx, OPGPU_E_STATE, "opgpu_finalize_initialization: already initialized");
+    grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
+        ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 0);
+    CK(cudaGetLastError());
+    const uint32_t st = read_status(ctx);
+    if (st & OPGPU_E_CUDA) return st;
+    ctx->initialized = true;
+    return st & OPGPU_SOFT_MASK;
+}
+
+static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_step: call opgpu_finalize_initialization first")) return r;
+    if (nsteps < 0 || !(dt > 0.0)) return fail(ctx, OPGPU_E_INVALID, "opgpu_step: dt > 0 and nsteps >= 0 required");
+    if (ctx->sp.use_dg && !ctx->d_dg) return fail(ctx, OPGPU_E_STATE, "opgpu_step: driving force enabled without values");
+    StepParams sp = ctx->sp;
+    sp.dt = dt;
+    for (int s = 0; s < nsteps; s++)
+    {
+        const int in = ctx->cur, out = 1 - ctx->cur;
+        StepArrays a{};
+        a.cnt_in = ctx->cnt[in]; a.idx_in = ctx->idx[in]; a.val_in = ctx->val[in];
+        a.cnt_out = ctx->cnt[out]; a.idx_out = ctx->idx[out]; a.val_out = ctx->val[out];
+        a.vr = ctx->d_vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
+        a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
+        a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
+        const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->stream)
+                                 : launch_step_f64(sp, a, ctx->K, ctx->stream);
+        if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("step launch: ") + cudaGetErrorString((cudaError_t)rc));
+        grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
+            ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 1);
+        CK(cudaGetLastError());
+        ctx->cur = out;
+    }
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_step_async(opgpu_ctx* ctx, double dt, int32_t nsteps)
+{
+    return enqueue_steps(ctx, dt, nsteps);
+}
+
+extern "C" uint32_t opgpu_sync(opgpu_ctx* ctx)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    const uint32_t st = read_status(ctx);
+    if (st & OPGPU_E_CUDA) return st;
+    return st & OPGPU_SOFT_MASK;
+}
+
+extern "C" uint32_t opgpu_step(opgpu_ctx* ctx, double dt, int32_t nsteps)
+{
+    if (uint32_t r = enqueue_steps(ctx, dt, nsteps)) return r;
+    return opgpu_sync(ctx);
+}
+
+extern "C" uint32_t opgpu_total_entries(opgpu_ctx* ctx, int64_t* total)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded, "no state")) return r;
+    if (!total) return OPGPU_E_INVALID;
+    const long long N = ctx->n;
+    int32_t* d_counts = nullptr;
+    long long *d_sum = nullptr, *d_wide = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    CK(dalloc(&d_counts, N));
+    CK(dalloc(&d_wide, N));
+    CK(dalloc(&d_sum, 1));
+    counts_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], d_counts, d_wide);
+    CK(cub::DeviceReduce::Sum(nullptr, tmp_bytes, d_wide, d_sum, N, ctx->stream));
+    CK(cudaMalloc(&d_tmp, tmp_bytes + 16));
+    CK(cub::DeviceReduce::Sum(d_tmp, tmp_bytes, d_wide, d_sum, N, ctx->stream));
+    long long t = 0;
+    CK(cudaMemcpyAsync(&t, d_sum, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    dfree(d_counts); dfree(d_wide); dfree(d_sum); dfree(d_tmp);
+    *total = t;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_download_lists(opgpu_ctx* ctx, int32_t* counts, int32_t* idx, double* val)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded, "no state")) return r;
+    if (!counts || !idx || !val) return OPGPU_E_INVALID;
+    const long long N = ctx->n;
+    int64_t total = 0;
+    if (uint32_t r = opgpu_total_entries(ctx, &total)) return r;
+    int32_t *d_counts = nullptr, *d_idx = nullptr;
+    long long *d_off = nullptr, *d_wide = nullptr;
+    double* d_val = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    CK(dalloc(&d_counts, N));
+    CK(dalloc(&d_off, N));
+    CK(dalloc(&d_wide, N));
+    CK(dalloc(&d_idx, total));
+    CK(dalloc(&d_val, total));
+    counts_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], d_counts, d_wide);
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_wide, d_off, N, ctx->stream));
+    CK(cudaMalloc(&d_tmp, tmp_bytes + 16));
+    CK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_wide, d_off, N, ctx->stream));
+    if (ctx->fp32)
+        gather_kernel<float><<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], ctx->idx[ctx->cur],
+            static_cast<const float*>(ctx->val[ctx->cur]), d_off, d_idx, d_val);
+    else
+        gather_kernel<double><<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], ctx->idx[ctx->cur],
+            static_cast<const double*>(ctx->val[ctx->cur]), d_off, d_idx, d_val);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(counts, d_counts, N * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(idx, d_idx, total * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(val, d_val, total * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    dfree(d_counts); dfree(d_off); dfree(d_wide); dfree(d_idx); dfree(d_val); dfree(d_tmp);
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_download_flags(opgpu_ctx* ctx, int8_t* flags)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded, "no state")) return r;
+    if (!flags) return OPGPU_E_INVALID;
+    const long long N = ctx->n;
+    int8_t* d_flags = nullptr;
+    CK(dalloc(&d_flags, N));
+    flags_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(ctx->grid.nx, ctx->grid.ny, ctx->grid.nz,
+                                                             ctx->cnt[ctx->cur], d_flags);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(flags, d_flags, N, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    dfree(d_flags);
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_write_raw(opgpu_ctx* ctx, const char* path)
+{
+    if (!ctx || !path) return OPGPU_E_INVALID;
+    int64_t total = 0;
+    if (uint32_t r = opgpu_total_entries(ctx, &total)) return r;
+    std::vector<int32_t> counts(ctx->n), idx(total);
+    std::vector<double> val(total);
+    if (uint32_t r = opgpu_download_lists(ctx, counts.data(), idx.data(), val.data())) return r;
+    std::string err;
+    if (!raw_write(path, ctx->grid.nx, ctx->grid.ny, ctx->grid.nz, counts.data(), idx.data(), val.data(), err))
+        return fail(ctx, OPGPU_E_IO, err);
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_grains(opgpu_ctx* ctx, double* volume, double* volume_ratio, double* max_volume,
+                                 int32_t* exist, int32_t* stage)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "no grains")) return r;
+    const int G = ctx->G;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (volume) CK(cudaMemcpy(volume, ctx->d_volume, G * sizeof(double), cudaMemcpyDeviceToHost));
+    if (volume_ratio) CK(cudaMemcpy(volume_ratio, ctx->d_vr, G * sizeof(double), cudaMemcpyDeviceToHost));
+    if (max_volume) CK(cudaMemcpy(max_volume, ctx->d_maxvol, G * sizeof(double), cudaMemcpyDeviceToHost));
+    if (exist || stage)
+    {
+        std::vector<int8_t> tmp(G);
+        if (exist)
+        {
+            CK(cudaMemcpy(tmp.data(), ctx->d_exist, G, cudaMemcpyDeviceToHost));
+            for (int g = 0; g < G; g++) exist[g] = tmp[g];
+        }
+        if (stage)
+        {
+            CK(cudaMemcpy(tmp.data(), ctx->d_gstage, G, cudaMemcpyDeviceToHost));
+            for (int g = 0; g < G; g++) stage[g] = tmp[g];
+        }
+    }
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    if (!stats) return OPGPU_E_INVALID;
+    unsigned long long c[kNumCounters];
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    read_status(ctx);
+    stats->steps = (int64_t)c[kCntSteps];
+    stats->wide_last = (int64_t)c[kCntWideLast];
+    stats->wide_total = (int64_t)c[kCntWideTotal];
+    stats->entries_in_total = (int64_t)c[kCntEntriesInTotal];
+    stats->entries_out_total = (int64_t)c[kCntEntriesOutTotal];
+    stats->status = ctx->status;
+    stats->overflow_voxels = (uint32_t)c[kCntOverflowVoxels];
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_clear_status(opgpu_ctx* ctx)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    read_status(ctx);
+    ctx->status = 0;
+    return OPGPU_OK;
+}

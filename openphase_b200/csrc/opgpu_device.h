@@ -1,0 +1,86 @@
+// Device-side data layout and launch interface of the fused multiphase-field step.
+//
+// State (one buffer of a ping-pong pair), structure of arrays over N = nx*ny*nz voxels:
+//   cnt[N]        uint8   number of stored (positive) fields of the voxel
+//   idx[K][N]     int16   grain index of slot s        (slot plane s at idx + s*N)
+//   val[K][N]     real    phase-field value of slot s  (real = double or float)
+// Slots s >= cnt[v] are never read.  Only positive entries are stored (what NodePF holds after
+// NodePF::finalize); the zero-valued candidate entries the reference appends in
+// CalculateDerivativesSR are re-derived inside the step kernel from the 3x3x3 neighbourhood.
+// A voxel's interface flag is never stored: flag = 2 if cnt > 1, else 1 if any of its 26 periodic
+// neighbours has cnt > 1, else 0 (identical to NodePF::finalize + PhaseField::SetFlagsSR).
+#pragma once
+#include <stdint.h>
+
+namespace opgpu {
+
+constexpr int kMaxPhases = 8;
+
+enum : uint32_t {
+    kStOverflowK = 1u << 0,
+    kStOverflowList = 1u << 1,
+    kStEmptyVoxel = 1u << 2,
+    kStNormalizeWarn = 1u << 3,
+    kStLimiterCap = 1u << 4,
+    kStNonFinite = 1u << 5,
+};
+
+// counters[] slots: the step kernel adds into the per-step slots 0-2; the grain-update kernel rolls
+// them into the running totals and clears them.
+enum {
+    kCntWide = 0, kCntEntriesIn = 1, kCntEntriesOut = 2, kCntOverflowVoxels = 3,
+    kCntWideTotal = 4, kCntEntriesInTotal = 5, kCntEntriesOutTotal = 6, kCntWideLast = 7, kCntSteps = 8,
+    kNumCounters = 9
+};
+
+struct StepParams {
+    int nx, ny, nz;
+    long long n;
+    // Laplacian stencil (LaplacianStencil::Set order) and the neighbour set used to discover
+    // candidates after it (GradientStencil::Set order), both with periodic offsets.
+    int ns;
+    signed char lap_d[27][3];
+    double lap_w[27];
+    int ng;
+    signed char grad_d[27][3];
+    double pref_do;          // Pi^2/Eta^2 (DoubleObstacle.cpp:504)
+    double pref_df;          // Pi/Eta     (DrivingForce.cpp:507)
+    double dt;
+    double eps_snap;         // finalize snap/erase threshold (DBL_EPSILON in the FP64 form)
+    int nphases;
+    double sigma_p[kMaxPhases * kMaxPhases];
+    double mu_p[kMaxPhases * kMaxPhases];
+    double allowed_p[kMaxPhases * kMaxPhases];   // Limit*Prefactor*MaxEnergy*RegularizationFactor
+    int limiting;
+    double tj_factor;
+    int consider_nucleus_volume;
+    int pair_mode;           // OPGPU_PAIRS_*
+    unsigned long long hash_seed;
+    double hash_lo, hash_span;
+    int ngrains;
+    int use_dg;
+};
+
+struct StepArrays {
+    const uint8_t* cnt_in;
+    const int16_t* idx_in;
+    const void* val_in;
+    uint8_t* cnt_out;
+    int16_t* idx_out;
+    void* val_out;
+    const double* vr;          // [G] VolumeRatio
+    const int16_t* gphase;     // [G]
+    const int8_t* gstage;      // [G]
+    const double* dg;          // [G] or null
+    const double* pair_sigma;  // [G*G] or null
+    const double* pair_mu;     // [G*G] or null
+    double* vol_acc;           // [G] volume accumulator of the output state (zeroed by the caller)
+    uint32_t* status;          // soft status bits
+    unsigned long long* counters;  // kNumCounters
+};
+
+// Launchers (defined in step_f64.cu / step_f32.cu).  k_slots in {8, 12, 16}.
+int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
+int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
+
+}  // namespace opgpu

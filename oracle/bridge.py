@@ -1,0 +1,210 @@
+"""TEST INFRASTRUCTURE ONLY — Python access to the checkers.
+
+* `Oracle`        ctypes wrapper of liboracle.so, the C restatement of the reference step
+* `run_reference` runs the unmodified reference (oracle/_ref/ref_driver, built from the reference
+                  sources by oracle/Makefile) on a case and returns its dumped states
+
+Only the tests, the smoke check and the bench's CPU-baseline / reference legs import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_DRIVER = HERE / "_ref" / "ref_driver"
+STENCIL = {"SIMPLE": 0, "ISOTROPIC": 1, "LB": 2}
+
+S_LIST_OVERFLOW, S_EMPTY_VOXEL, S_NORMALIZE_WARN, S_LIMITER_CAP = 1, 2, 4, 8
+
+
+class OpParams(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dx", C.c_double), ("iwidth", C.c_double),
+                ("stencil", C.c_int), ("gradient_stencil", C.c_int), ("nphases", C.c_int), ("ngrains", C.c_int),
+                ("grain_phase", C.c_void_p), ("phase_solid", C.c_void_p), ("sigma_phase", C.c_void_p),
+                ("mu_phase", C.c_void_p), ("energy_model", C.c_void_p), ("cubic_eps", C.c_void_p),
+                ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
+                ("limiting", C.c_int), ("limit_phase", C.c_void_p), ("regularization", C.c_double),
+                ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int),
+                ("nucleus_volume_factor", C.c_double), ("threads", C.c_int)]
+
+
+_olib = None
+
+
+def build_oracle():
+    """Compile liboracle.so (and the reference build when the reference sources are present)."""
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True, env=env)
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        if not ORACLE_LIB.exists():
+            build_oracle()
+        L = C.CDLL(str(ORACLE_LIB))
+        L.op_create.restype = C.c_void_p
+        L.op_create.argtypes = [C.POINTER(OpParams), C.c_int]
+        L.op_destroy.argtypes = [C.c_void_p]
+        L.op_load.restype = C.c_int
+        L.op_load.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.op_finalize_initialization.argtypes = [C.c_void_p]
+        L.op_step.restype = C.c_uint32
+        L.op_step.argtypes = [C.c_void_p, C.c_double, C.c_int]
+        L.op_total_entries.restype = C.c_long
+        L.op_total_entries.argtypes = [C.c_void_p]
+        L.op_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.op_get_flags.argtypes = [C.c_void_p, C.c_void_p]
+        L.op_wide_count.restype = C.c_long
+        L.op_wide_count.argtypes = [C.c_void_p]
+        L.op_get_grains.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        L.op_set_grains.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        _olib = L
+    return _olib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Oracle:
+    """The C restatement of the reference step, loaded with a case's initial state."""
+
+    def __init__(self, case, counts, idx, val, cap=32, threads=0):
+        L = oracle_lib()
+        self._keep = []
+
+        def keep(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a)
+            self._keep.append(a)
+            return a
+
+        G = case.ngrains
+        sig = keep(np.array([[case.sigma]], dtype=np.float64))
+        mu = keep(np.array([[case.mu]], dtype=np.float64))
+        lim = keep(np.array([[case.limit]], dtype=np.float64))
+        ps = case.pair_sigma()
+        ps = keep(ps.astype(np.float64)) if ps is not None else None
+        dg = case.driving_force()
+        dg = keep(dg) if dg is not None else None
+        p = OpParams(nx=case.nx, ny=case.ny, nz=case.nz, dx=case.dx, iwidth=case.iwidth,
+                     stencil=STENCIL[case.stencil], gradient_stencil=STENCIL[case.gradient_stencil],
+                     nphases=1, ngrains=G, grain_phase=None, phase_solid=None,
+                     sigma_phase=_p(sig).value, mu_phase=_p(mu).value, energy_model=None, cubic_eps=None,
+                     quat=None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
+                     dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
+                     limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
+                     consider_nucleus_volume=1, nucleus_volume_factor=1.0, threads=threads)
+        self.case = case
+        self.h = L.op_create(C.byref(p), cap)
+        if not self.h:
+            raise RuntimeError("op_create failed")
+        counts = np.ascontiguousarray(counts, dtype=np.int32)
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        if L.op_load(self.h, _p(counts), _p(idx), _p(val)) != 0:
+            raise RuntimeError("op_load: list longer than the oracle capacity")
+        L.op_finalize_initialization(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            oracle_lib().op_destroy(self.h)
+            self.h = None
+
+    def step(self, nsteps, dt=None):
+        return int(oracle_lib().op_step(self.h, self.case.dt if dt is None else dt, nsteps))
+
+    def state(self):
+        L = oracle_lib()
+        n = self.case.n
+        total = L.op_total_entries(self.h)
+        counts = np.empty(n, dtype=np.int32)
+        idx = np.empty(total, dtype=np.int32)
+        val = np.empty(total, dtype=np.float64)
+        L.op_get_state(self.h, _p(counts), _p(idx), _p(val))
+        return counts, idx, val
+
+    def flags(self):
+        f = np.empty(self.case.n, dtype=np.int8)
+        oracle_lib().op_get_flags(self.h, _p(f))
+        return f
+
+    def wide_count(self):
+        return int(oracle_lib().op_wide_count(self.h))
+
+    def grains(self):
+        G = self.case.ngrains
+        vol, vr, mx = (np.empty(G) for _ in range(3))
+        ex, st = np.empty(G, dtype=np.int32), np.empty(G, dtype=np.int32)
+        oracle_lib().op_get_grains(self.h, _p(vol), _p(vr), _p(mx), _p(ex), _p(st))
+        return {"volume": vol, "volume_ratio": vr, "max_volume": mx, "exist": ex, "stage": st}
+
+
+def reference_available() -> bool:
+    return REF_DRIVER.exists()
+
+
+def _case_text(case, workdir: Path, dump_steps, threads):
+    lines = [f"nx {case.nx}", f"ny {case.ny}", f"nz {case.nz}", f"dx {case.dx!r}", f"iwidth {case.iwidth!r}",
+             f"stencil {case.stencil}", f"dt {case.dt!r}", f"nsteps {max(dump_steps)}", "nphases 1",
+             f"sigma 0 0 {case.sigma!r}", f"mu 0 0 {case.mu!r}", f"limit 0 0 {case.limit!r}",
+             f"ngrains {case.ngrains}", f"limiting {int(case.limiting)}",
+             f"regularization {case.regularization!r}", f"tj_factor {case.tj_factor!r}",
+             "dump_steps " + " ".join(str(s) for s in dump_steps)]
+    if threads:
+        lines.append(f"threads {threads}")
+    ps = case.pair_sigma()
+    if ps is not None:
+        f = workdir / "pair_sigma.bin"
+        np.ascontiguousarray(ps, dtype=np.float64).tofile(f)
+        lines.append(f"pair_sigma_file {f}")
+    dg = case.driving_force()
+    if dg is not None:
+        f = workdir / "dg.bin"
+        dg.astype(np.float64).tofile(f)
+        lines.append(f"dg_file {f}")
+    return "\n".join(lines) + "\n"
+
+
+def run_reference(case, counts, idx, val, dump_steps, threads=0, workdir=None):
+    """Run the compiled reference on the case; returns {step: (counts, idx, val, volume, volume_ratio)}
+    and the stats dictionary (wall time of the step loop, threads, wide-interface counts)."""
+    from openphase_b200.initializations import raw_bytes, parse_raw
+
+    if not REF_DRIVER.exists():
+        raise FileNotFoundError("reference driver not built (make -C oracle ref)")
+    tmp = tempfile.TemporaryDirectory() if workdir is None else None
+    wd = Path(workdir or tmp.name)
+    wd.mkdir(parents=True, exist_ok=True)
+    (wd / "case.txt").write_text(_case_text(case, wd, dump_steps, threads))
+    (wd / "init.dat").write_bytes(raw_bytes(case.nx, case.ny, case.nz, counts, idx, val))
+    out = wd / "out"
+    out.mkdir(exist_ok=True)
+    r = subprocess.run([str(REF_DRIVER), str(wd / "case.txt"), str(wd / "init.dat"), str(out)],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stderr[-2000:]}")
+    res = {}
+    for s in dump_steps:
+        _, c, i, v = parse_raw((out / f"PF_{s}.dat").read_bytes())
+        vol = np.fromfile(out / f"V_{s}.bin", dtype=np.float64)
+        vr = np.fromfile(out / f"VR_{s}.bin", dtype=np.float64)
+        res[s] = (c, i, v, vol, vr)
+    stats = {}
+    for line in (out / "stats.txt").read_text().splitlines():
+        k, *vals = line.split()
+        stats[k] = [float(x) for x in vals] if len(vals) > 1 else float(vals[0])
+    if tmp is not None:
+        tmp.cleanup()
+    return res, stats

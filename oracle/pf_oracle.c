@@ -1,0 +1,738 @@
+/* TEST INFRASTRUCTURE ONLY — the oracle (see pf_oracle.h).
+ *
+ * A plain-C restatement of the OpenPhase single-resolution multiphase-field step.  Every function
+ * below names the reference function it restates (paths relative to the OpenPhase source tree).
+ * The operation order of every floating-point expression follows the reference statement by
+ * statement, so that in IEEE double arithmetic without FMA contraction (built with
+ * -ffp-contract=off) the results are bit-identical to the reference's own release build.
+ *
+ * Storage: one fixed-capacity list per voxel of (index, value, laplacian) entries, the analogue of
+ * NodePF (include/Containers/NodePF.h:40-180).  The per-voxel increment store FieldsDot
+ * (NodeAB<double,double>, include/Containers/NodeAB.h:38-180) lives in per-thread scratch,
+ * because every stage between CalculatePhaseFieldIncrements and NodePF::finalize only reads and
+ * writes the voxel's own lists; the grid-wide passes (flags, derivatives, volumes) run after the
+ * per-voxel stages exactly as in PhaseField::FinalizeSR (src/PhaseField.cpp:1008-1033).
+ */
+#include "pf_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* include/Globals.h:124 */
+static const double OP_PI = 3.14159265358979323846;
+
+typedef struct { int32_t idx; double val; double lap; double grad[3]; } entry;
+typedef struct { int a, b; double v1; int alive; } pair;
+
+struct op_sim {
+    op_params p;
+    int* grain_phase;
+    int* phase_solid;
+    double *sigma_phase, *mu_phase, *limit_phase, *pair_sigma, *pair_mu, *dg;
+    long n;
+    int cap;
+    int32_t* cnt;   entry* e;     /* Fields                                */
+    int32_t* cnt2;  entry* e2;    /* tmpFields of CalculateDerivativesSR   */
+    int8_t* flag;
+    double *volume, *max_volume, *ref_volume, *vr;
+    int32_t *exist, *stage;
+    int ns; int sdi[27], sdj[27], sdk[27]; double sw[27];
+    int ng; int gdi[27], gdj[27], gdk[27]; double gw[27][3];
+    uint32_t status;
+};
+
+static double dmax(double a, double b) { return (a < b) ? b : a; }   /* std::max */
+static double dmin(double a, double b) { return (b < a) ? b : a; }   /* std::min */
+
+static double* dup_d(const double* src, size_t n)
+{
+    if (!src) return NULL;
+    double* d = (double*)malloc(n * sizeof(double));
+    memcpy(d, src, n * sizeof(double));
+    return d;
+}
+
+/* LaplacianStencil::Set (include/Containers/LaplacianStencil.h:197-219) over the 3-D tables
+ * LaplacianStencil3D_7 (:72-82), LaplacianStencil3D_27a (:109-119), LaplacianStencil3D_LB
+ * (:146-156): elements in x, y, z loop order, zero weights skipped, weight = table/(dx*dx). */
+static void set_stencil(op_sim* s)
+{
+    double t[3][3][3];
+    const int st = s->p.stencil;
+    for (int x = 0; x < 3; x++)
+    for (int y = 0; y < 3; y++)
+    for (int z = 0; z < 3; z++)
+    {
+        const int d = (x != 1) + (y != 1) + (z != 1);
+        double w = 0.0;
+        if (st == OP_STENCIL_SIMPLE)
+            w = (d == 0) ? -6.0 : (d == 1 ? 1.0 : 0.0);
+        else if (st == OP_STENCIL_ISOTROPIC)
+            w = (d == 0) ? -64.0/15.0 : (d == 1 ? 7.0/15.0 : (d == 2 ? 1.0/10.0 : 1.0/30.0));
+        else
+            w = (d == 0) ? -38.0/9.0 : (d == 1 ? 4.0/9.0 : (d == 2 ? 1.0/9.0 : 1.0/36.0));
+        t[x][y][z] = w;
+    }
+    s->ns = 0;
+    for (int x = -1; x <= 1; ++x)
+    for (int y = -1; y <= 1; ++y)
+    for (int z = -1; z <= 1; ++z)
+    if (t[x+1][y+1][z+1] != 0.0)
+    {
+        s->sdi[s->ns] = x; s->sdj[s->ns] = y; s->sdk[s->ns] = z;
+        s->sw[s->ns] = t[x+1][y+1][z+1]/(s->p.dx*s->p.dx);
+        s->ns++;
+    }
+    /* GradientStencil::Set (include/Containers/GradientStencil.h:132-155) over GradientStencil1D
+     * (:46-56), GradientStencil3D (:82-92) and GradientStencil3D_LB (:108-118):
+     * weight_c = c*table/dx. */
+    const int gs = s->p.gradient_stencil;
+    for (int x = 0; x < 3; x++)
+    for (int y = 0; y < 3; y++)
+    for (int z = 0; z < 3; z++)
+    {
+        const int d = (x != 1) + (y != 1) + (z != 1);
+        double w = 0.0;
+        if (gs == OP_STENCIL_SIMPLE)
+            w = (d == 1) ? 0.5 : 0.0;
+        else if (gs == OP_STENCIL_ISOTROPIC)
+            w = (d == 0) ? 0.0 : (d == 1 ? 1.0/4.64 : (d == 2 ? 0.245/4.64 : 0.085/4.64));
+        else
+            w = (d == 0) ? 0.0 : (d == 1 ? 2.0/9.0 : (d == 2 ? 1.0/18.0 : 1.0/72.0));
+        t[x][y][z] = w;
+    }
+    s->ng = 0;
+    for (int x = -1; x <= 1; ++x)
+    for (int y = -1; y <= 1; ++y)
+    for (int z = -1; z <= 1; ++z)
+    if (t[x+1][y+1][z+1] != 0.0)
+    {
+        s->gdi[s->ng] = x; s->gdj[s->ng] = y; s->gdk[s->ng] = z;
+        s->gw[s->ng][0] = x*t[x+1][y+1][z+1]/s->p.dx;
+        s->gw[s->ng][1] = y*t[x+1][y+1][z+1]/s->p.dx;
+        s->gw[s->ng][2] = z*t[x+1][y+1][z+1]/s->p.dx;
+        s->ng++;
+    }
+}
+
+op_sim* op_create(const op_params* p, int cap)
+{
+    if (cap < 2 || cap > 64) return NULL;
+    op_sim* s = (op_sim*)calloc(1, sizeof(op_sim));
+    s->p = *p;
+    const int G = p->ngrains, P = p->nphases;
+    s->grain_phase = (int*)malloc(G * sizeof(int));
+    for (int g = 0; g < G; g++) s->grain_phase[g] = p->grain_phase ? p->grain_phase[g] : 0;
+    s->phase_solid = (int*)malloc(P * sizeof(int));
+    for (int q = 0; q < P; q++) s->phase_solid[q] = p->phase_solid ? p->phase_solid[q] : 1;
+    s->sigma_phase = dup_d(p->sigma_phase, (size_t)P*P);
+    s->mu_phase    = dup_d(p->mu_phase, (size_t)P*P);
+    s->limit_phase = dup_d(p->limit_phase, (size_t)P*P);
+    s->pair_sigma  = dup_d(p->pair_sigma, (size_t)G*G);
+    s->pair_mu     = dup_d(p->pair_mu, (size_t)G*G);
+    s->dg          = dup_d(p->dg, (size_t)G);
+    s->p.grain_phase = s->grain_phase; s->p.phase_solid = s->phase_solid;
+    s->p.sigma_phase = s->sigma_phase; s->p.mu_phase = s->mu_phase; s->p.limit_phase = s->limit_phase;
+    s->p.pair_sigma = s->pair_sigma; s->p.pair_mu = s->pair_mu; s->p.dg = s->dg;
+    s->p.energy_model = NULL; s->p.cubic_eps = NULL; s->p.quat = NULL;
+    if (s->p.nucleus_volume_factor == 0.0) s->p.nucleus_volume_factor = 1.0;
+    s->n = (long)p->nx * p->ny * p->nz;
+    s->cap = cap;
+    s->cnt  = (int32_t*)calloc(s->n, sizeof(int32_t));
+    s->cnt2 = (int32_t*)calloc(s->n, sizeof(int32_t));
+    s->e  = (entry*)calloc((size_t)s->n * cap, sizeof(entry));
+    s->e2 = (entry*)calloc((size_t)s->n * cap, sizeof(entry));
+    s->flag = (int8_t*)calloc(s->n, 1);
+    s->volume = (double*)calloc(G, sizeof(double));
+    s->max_volume = (double*)calloc(G, sizeof(double));
+    s->ref_volume = (double*)calloc(G, sizeof(double));
+    s->vr = (double*)calloc(G, sizeof(double));
+    s->exist = (int32_t*)calloc(G, sizeof(int32_t));
+    s->stage = (int32_t*)calloc(G, sizeof(int32_t));
+    /* PhaseField::AddGrainInfo (src/PhaseField.cpp:2970-2979) on a fresh Grain
+     * (include/GrainsProperties.h:312-336, add_grain :708-730), and
+     * PhaseField::CalculateReferenceVolume (src/PhaseField.cpp:367-391) in 3-D. */
+    const double r = p->iwidth;
+    const double ref = (4.0/3.0)*OP_PI*r*r*r*s->p.nucleus_volume_factor;
+    for (int g = 0; g < G; g++)
+    {
+        s->exist[g] = 1; s->stage[g] = OP_STAGE_STABLE;
+        s->ref_volume[g] = ref; s->vr[g] = 0.0;
+    }
+    set_stencil(s);
+    if (p->threads > 0) omp_set_num_threads(p->threads);
+    return s;
+}
+
+void op_destroy(op_sim* s)
+{
+    if (!s) return;
+    free(s->grain_phase); free(s->phase_solid);
+    free(s->sigma_phase); free(s->mu_phase); free(s->limit_phase);
+    free(s->pair_sigma); free(s->pair_mu); free(s->dg);
+    free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
+    free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
+    free(s->exist); free(s->stage);
+    free(s);
+}
+
+static long vox(const op_sim* s, int i, int j, int k)
+{
+    /* periodic wrap; storage order of Storage3D (include/Containers/Storage3D.h:2054-2064):
+     * x slowest, z fastest */
+    const int nx = s->p.nx, ny = s->p.ny, nz = s->p.nz;
+    i = (i + nx) % nx; j = (j + ny) % ny; k = (k + nz) % nz;
+    return ((long)i * ny + j) * nz + k;
+}
+
+/* NodePF::read (include/Containers/NodePF.h:751-763): flag 2 when more than one entry. */
+int op_load(op_sim* s, const int32_t* counts, const int32_t* idx, const double* val)
+{
+    long off = 0;
+    for (long v = 0; v < s->n; v++)
+    {
+        const int c = counts[v];
+        if (c > s->cap) return -1;
+        s->cnt[v] = c;
+        s->flag[v] = (c > 1) ? 2 : 0;
+        for (int q = 0; q < c; q++)
+        {
+            s->e[v*s->cap + q].idx = idx[off + q];
+            s->e[v*s->cap + q].val = val[off + q];
+            s->e[v*s->cap + q].lap = 0.0;
+            s->e[v*s->cap + q].grad[0] = 0.0;
+            s->e[v*s->cap + q].grad[1] = 0.0;
+            s->e[v*s->cap + q].grad[2] = 0.0;
+        }
+        off += c;
+    }
+    return 0;
+}
+
+/* ---------------- interface properties (InterfaceProperties::SetSR, src/InterfaceProperties.cpp:603-762)
+ * ISO energy model (:617-620) and ISO mobility (:677-680, MaxMobility = Mobility); a per-grain-pair
+ * table replaces the per-voxel values the way the oracle driver writes them into IP.Properties. */
+static double ip_energy(const op_sim* s, int ga, int gb)
+{
+    if (s->pair_sigma) return s->pair_sigma[(size_t)ga*s->p.ngrains + gb];
+    const int P = s->p.nphases;
+    return s->sigma_phase[s->grain_phase[ga]*P + s->grain_phase[gb]];
+}
+static double ip_mobility(const op_sim* s, int ga, int gb)
+{
+    if (s->pair_mu) return s->pair_mu[(size_t)ga*s->p.ngrains + gb];
+    const int P = s->p.nphases;
+    return s->mu_phase[s->grain_phase[ga]*P + s->grain_phase[gb]];
+}
+static double phase_energy(const op_sim* s, int pa, int pb)
+{
+    return s->sigma_phase[pa*s->p.nphases + pb];
+}
+
+/* PhaseField::LocalN (include/PhaseField.h:84-95) */
+static double local_n(const op_sim* s, const entry* L, int n)
+{
+    if (!s->p.consider_nucleus_volume) return (double)n;
+    double norm = 0.0;
+    for (int a = 0; a < n; a++) norm += s->vr[L[a].idx];
+    return norm;
+}
+
+/* pair position for a < b in a list of n entries (DO creates the pairs in this order) */
+static int pair_pos(int a, int b, int n)
+{
+    return a*(2*n - a - 1)/2 + (b - a - 1);
+}
+
+/* NodeAB::get_asym1 (include/Containers/NodeAB.h:517-531) for the list positions a != b. */
+static double get_asym1(const pair* P, int a, int b, int n)
+{
+    if (a < b) { const pair* q = &P[pair_pos(a, b, n)]; return q->alive ? q->v1 : 0.0; }
+    const pair* q = &P[pair_pos(b, a, n)];
+    return q->alive ? q->v1*(-1.0) : 0.0;
+}
+
+/* DoubleObstacle::CalculatePhaseFieldIncrementsSR (src/DoubleObstacle.cpp:502-571), one voxel. */
+static int do_increments(const op_sim* s, const entry* L, int n, pair* P)
+{
+    const double Eta = s->p.iwidth*s->p.dx;             /* src/GridParameters.cpp:256 */
+    const double Prefactor = OP_PI*OP_PI/(Eta*Eta);
+    const double norm_1 = 1.0/local_n(s, L, n);
+    int np = 0;
+    for (int a = 0; a < n; a++)
+    for (int b = a + 1; b < n; b++)
+    {
+        const int ga = L[a].idx, gb = L[b].idx;
+        const double scale = sqrt(s->vr[ga]*s->vr[gb]);
+        double dPhi_dt = ip_energy(s, ga, gb)
+                         *((L[a].lap + 0.5*(1.0 + scale)*Prefactor*L[a].val) -
+                           (L[b].lap + 0.5*(1.0 + scale)*Prefactor*L[b].val));
+        if (n > 2)
+        for (int c = 0; c < n; c++)
+        if (c != a && c != b)
+        {
+            const int gc = L[c].idx;
+            dPhi_dt += (ip_energy(s, gb, gc) - ip_energy(s, ga, gc))
+                      *(L[c].lap + 0.5*(1.0 + scale)*Prefactor*L[c].val);
+            /* TripleJunctionModels::Model (:536-552) */
+            if (s->p.tj_factor != 0.0 || scale < 1.0)
+            {
+                const int pA = s->grain_phase[ga], pB = s->grain_phase[gb], pG = s->grain_phase[gc];
+                dPhi_dt += dmax(s->p.tj_factor, (1.0 - scale))*Prefactor
+                               *(phase_energy(s, pA, pB) + phase_energy(s, pB, pG) + phase_energy(s, pA, pG))
+                               *(L[a].val*L[c].val - L[b].val*L[c].val);
+            }
+        }
+        dPhi_dt *= ip_mobility(s, ga, gb)*norm_1*scale;
+        /* NodeAB::add_asym1 on an empty FieldsDot creates the entry (NodeAB.h:467-490) */
+        P[np].a = a; P[np].b = b; P[np].v1 = dPhi_dt; P[np].alive = 1;
+        np++;
+    }
+    return np;
+}
+
+/* DrivingForce::MergePhaseFieldIncrementsSR (src/DrivingForce.cpp:497-602) after SkipAverage
+ * (:258-274) with $Average No, for the per-grain driving force raw(a,b) = dG_b - dG_a that the
+ * oracle driver adds with NodeDF::add_raw for each pair (a before b) of an interface voxel. */
+static void df_merge(const op_sim* s, const entry* L, int n, pair* P)
+{
+    const double Eta = s->p.iwidth*s->p.dx;
+    const double Prefactor = OP_PI/Eta;
+    const int NP = s->p.nphases;
+    for (int a = 0; a < n; a++)
+    for (int b = a + 1; b < n; b++)
+    {
+        const int ga = L[a].idx, gb = L[b].idx;
+        double locdG = s->dg[gb] - s->dg[ga];
+        double norm = sqrt(L[a].val*L[b].val);
+        if (s->stage[ga] == OP_STAGE_SEED || s->stage[gb] == OP_STAGE_SEED) norm += 1.0e-6;
+        if (s->p.limiting)
+        {
+            const int pA = s->grain_phase[ga], pB = s->grain_phase[gb];
+            const double lim = s->limit_phase ? s->limit_phase[pA*NP + pB] : 0.95;
+            double allowedDG = lim*Prefactor*phase_energy(s, pA, pB);   /* ISO: MaxEnergy = Energy */
+            allowedDG *= s->p.regularization;
+            locdG = allowedDG*tanh(locdG/allowedDG);
+        }
+        const double dPsi_dt = locdG*ip_mobility(s, ga, gb)*norm*Prefactor;
+        P[pair_pos(a, b, n)].v1 += dPsi_dt;
+    }
+}
+
+/* PhaseField::NormalizeIncrementsSR (src/PhaseField.cpp:1351-1561), one voxel. */
+static uint32_t normalize(const entry* L, int n, pair* P, int np, double dt)
+{
+    uint32_t st = 0;
+    const double precision = FLT_EPSILON;
+    if (np == 0) return 0;
+    if (np == 1)
+    {
+        /* :1368-1404 — the single pair's first index is list entry 0 */
+        const double valueA = (P[0].v1 + 0.0)*dt;
+        const double old_value = L[P[0].a].val;
+        if ((old_value == 0.0 && valueA < 0.0) || (old_value == 1.0 && valueA > 0.0))
+        {
+            P[0].alive = 0;
+        }
+        else
+        {
+            const double new_value = old_value + valueA;
+            double norm = 1.0;
+            if (new_value < 0.0)      norm *= -old_value/valueA;
+            else if (new_value > 1.0) norm *= (1.0 - old_value)/valueA;
+            if (norm > DBL_EPSILON) P[0].v1 *= norm;
+            else P[0].alive = 0;
+        }
+        return 0;
+    }
+    /* :1407-1431 zero all pairs of a field that would leave [0,1] */
+    for (int a = 0; a < n; a++)
+    {
+        double dPsiAlpha = 0.0;
+        for (int b = 0; b < n; b++)
+        if (a != b)
+        {
+            dPsiAlpha += get_asym1(P, a, b, n);
+        }
+        if ((L[a].val == 0.0 && dPsiAlpha < 0.0) || (L[a].val == 1.0 && dPsiAlpha > 0.0))
+        {
+            for (int b = 0; b < n; b++)
+            if (a != b)
+            {
+                pair* q = (a < b) ? &P[pair_pos(a, b, n)] : &P[pair_pos(b, a, n)];
+                q->v1 = 0.0;   /* set_sym_pair(.., 0, 0); an erased pair would be re-added as zero */
+            }
+        }
+    }
+    /* :1433-1445 erase zero pairs */
+    int nalive = 0;
+    for (int q = 0; q < np; q++)
+    {
+        if (P[q].alive && P[q].v1 == 0.0) P[q].alive = 0;
+        nalive += P[q].alive;
+    }
+    if (!nalive) return 0;
+    /* :1447-1519 iterative limiting */
+    double pos[64], neg[64], limP[64], limN[64];
+    int iterations = 0;
+    int limiting_needed = 1;
+    while (limiting_needed)
+    {
+        iterations++;
+        limiting_needed = 0;
+        for (int a = 0; a < n; a++) { pos[a] = 0.0; neg[a] = 0.0; }
+        for (int q = 0; q < np; q++)
+        if (P[q].alive)
+        {
+            const double v = P[q].v1;
+            if (v < 0.0) { neg[P[q].a] += v; pos[P[q].b] += -v; }
+            if (v > 0.0) { pos[P[q].a] += v; neg[P[q].b] += -v; }
+        }
+        for (int a = 0; a < n; a++)
+        {
+            const double newPFvalue = L[a].val + (pos[a] + neg[a])*dt;
+            limN[a] = 1.0;
+            limP[a] = 1.0;
+            if (newPFvalue < 0.0)
+                limN[a] = dmin(1.0, -(L[a].val + pos[a]*dt)/(neg[a]*dt));
+            if (newPFvalue > 1.0)
+                limP[a] = dmin(1.0, (1.0 - (L[a].val + neg[a]*dt))/(pos[a]*dt));
+        }
+        for (int q = 0; q < np; q++)
+        if (P[q].alive)
+        {
+            if (P[q].v1 < 0.0)
+            {
+                const double lim = dmin(limN[P[q].a], limP[P[q].b]);
+                P[q].v1 *= lim;
+                if (lim < 1.0) limiting_needed = 1;
+            }
+            if (P[q].v1 > 0.0)
+            {
+                const double lim = dmin(limP[P[q].a], limN[P[q].b]);
+                P[q].v1 *= lim;
+                if (lim < 1.0) limiting_needed = 1;
+            }
+        }
+        if (iterations > 24)
+        {
+            if (limiting_needed) st |= OP_S_LIMITER_CAP;
+            limiting_needed = 0;
+        }
+    }
+    /* :1521-1533 erase increments below DBL_EPSILON */
+    for (int q = 0; q < np; q++)
+    if (P[q].alive && fabs(P[q].v1*dt) < DBL_EPSILON) P[q].alive = 0;
+    /* :1535-1561 plausibility check (warning only) */
+    double tmp[64];
+    for (int a = 0; a < n; a++) tmp[a] = L[a].val;
+    for (int q = 0; q < np; q++)
+    if (P[q].alive && P[q].v1 != 0.0)
+    {
+        tmp[P[q].a] += P[q].v1*dt;
+        tmp[P[q].b] += -P[q].v1*dt;
+    }
+    for (int a = 0; a < n; a++)
+    if (tmp[a] < -precision || tmp[a] > 1.0 + precision) st |= OP_S_NORMALIZE_WARN;
+    return st;
+}
+
+/* PhaseField::MergeIncrementsSR (src/PhaseField.cpp:1268-1299), one voxel; growth-constraint
+ * factor 1 (GrowthConstraintsViolations::None for every grain). */
+static void merge(entry* L, const pair* P, int np, double dt)
+{
+    for (int q = 0; q < np; q++)
+    if (P[q].alive)
+    {
+        const double factor = 1.0;
+        const double value = factor*(P[q].v1 + 0.0)*dt;
+        if (fabs(value) >= DBL_EPSILON)
+        {
+            L[P[q].a].val += value;
+            L[P[q].b].val += -value;
+        }
+    }
+}
+
+/* NodePF::finalize (include/Containers/NodePF.h:214-255); returns the new flag. */
+static int node_finalize(entry* L, int32_t* cnt, uint32_t* st)
+{
+    double total = 0.0;
+    int n = *cnt, m = 0;
+    for (int a = 0; a < n; a++)
+    {
+        int erase = 0;
+        if (L[a].val >= 1.0 - DBL_EPSILON) L[a].val = 1.0;
+        if (L[a].val <= 0.0 + DBL_EPSILON) { L[a].val = 0.0; erase = 1; }
+        total += L[a].val;
+        if (!erase) L[m++] = L[a];
+    }
+    *cnt = m;
+    if (m > 1)
+    {
+        const double norm = 1.0/total;
+        for (int a = 0; a < m; a++)
+        {
+            L[a].val *= norm; L[a].lap = 0.0;
+            L[a].grad[0] = 0.0; L[a].grad[1] = 0.0; L[a].grad[2] = 0.0;
+        }
+        return 2;
+    }
+    if (m == 0) { *st |= OP_S_EMPTY_VOXEL; return 0; }
+    L[0].val = 1.0;
+    L[0].lap = 0.0;
+    L[0].grad[0] = 0.0; L[0].grad[1] = 0.0; L[0].grad[2] = 0.0;
+    return 0;
+}
+
+/* PhaseField::SetFlagsSR (src/PhaseField.cpp:953-969) with periodic halos. */
+static void set_flags(op_sim* s)
+{
+    const int nx = s->p.nx, ny = s->p.ny, nz = s->p.nz;
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+    for (int k = 0; k < nz; k++)
+    {
+        const long v = ((long)i*ny + j)*nz + k;
+        if (s->flag[v] != 0) continue;
+        int f = 0;
+        for (int di = -1; di <= 1 && !f; di++)
+        for (int dj = -1; dj <= 1 && !f; dj++)
+        for (int dk = -1; dk <= 1 && !f; dk++)
+        if (s->flag[vox(s, i+di, j+dj, k+dk)] == 2) f = 1;
+        if (f) s->flag[v] = -1;   /* mark, resolved below so that marks do not propagate */
+    }
+    #pragma omp parallel for schedule(static)
+    for (long v = 0; v < s->n; v++) if (s->flag[v] == -1) s->flag[v] = 1;
+}
+
+/* PhaseField::CalculateDerivativesSR (src/PhaseField.cpp:566-615): Laplacian pass, then gradient
+ * pass, both appending zero-valued candidate entries for indices met in the neighbourhood;
+ * NodePF::set_temporary / add_laplacian_tmp / add_gradient_tmp / copy_from_temporary
+ * (NodePF.h:183-192, 351-366, 411-427). */
+static void calculate_derivatives(op_sim* s)
+{
+    const int nx = s->p.nx, ny = s->p.ny, nz = s->p.nz, cap = s->cap;
+    uint32_t st = 0;
+    #pragma omp parallel for collapse(2) schedule(static) reduction(|:st)
+    for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+    for (int k = 0; k < nz; k++)
+    {
+        const long v = ((long)i*ny + j)*nz + k;
+        if (s->flag[v] == 0) continue;
+        entry* T = s->e2 + v*cap;
+        int n = s->cnt[v];
+        memcpy(T, s->e + v*cap, n*sizeof(entry));
+        for (int q = 0; q < s->ns; q++)
+        {
+            const long u = vox(s, i + s->sdi[q], j + s->sdj[q], k + s->sdk[q]);
+            const entry* U = s->e + u*cap;
+            for (int r = 0; r < s->cnt[u]; r++)
+            if (U[r].val != 0.0)
+            {
+                const double laplacian = s->sw[q]*U[r].val;
+                int f = 0;
+                for (; f < n; f++) if (T[f].idx == U[r].idx) break;
+                if (f < n) T[f].lap += laplacian;
+                else if (n < cap)
+                {
+                    T[n].idx = U[r].idx; T[n].val = 0.0; T[n].lap = laplacian;
+                    T[n].grad[0] = 0.0; T[n].grad[1] = 0.0; T[n].grad[2] = 0.0;
+                    n++;
+                }
+                else st |= OP_S_LIST_OVERFLOW;
+            }
+        }
+        for (int q = 0; q < s->ng; q++)
+        {
+            const long u = vox(s, i + s->gdi[q], j + s->gdj[q], k + s->gdk[q]);
+            const entry* U = s->e + u*cap;
+            for (int r = 0; r < s->cnt[u]; r++)
+            if (U[r].val != 0.0)
+            {
+                const double gx = s->gw[q][0]*U[r].val;
+                const double gy = s->gw[q][1]*U[r].val;
+                const double gz = s->gw[q][2]*U[r].val;
+                int f = 0;
+                for (; f < n; f++) if (T[f].idx == U[r].idx) break;
+                if (f < n) { T[f].grad[0] += gx; T[f].grad[1] += gy; T[f].grad[2] += gz; }
+                else if (n < cap)
+                {
+                    T[n].idx = U[r].idx; T[n].val = 0.0; T[n].lap = 0.0;
+                    T[n].grad[0] = gx; T[n].grad[1] = gy; T[n].grad[2] = gz;
+                    n++;
+                }
+                else st |= OP_S_LIST_OVERFLOW;
+            }
+        }
+        s->cnt2[v] = n;
+    }
+    s->status |= st;
+    #pragma omp parallel for schedule(static)
+    for (long v = 0; v < s->n; v++)
+    if (s->flag[v] != 0)
+    {
+        s->cnt[v] = s->cnt2[v];
+        memcpy(s->e + v*cap, s->e2 + v*cap, s->cnt2[v]*sizeof(entry));
+    }
+}
+
+/* PhaseField::CalculateGrainsVolume (src/PhaseField.cpp:812-951), single process.  The volume sum
+ * runs over static per-thread chunks added in thread order (the reference adds per-thread partial
+ * arrays of a dynamic schedule; the two orders differ only in the last bits). */
+static void calculate_grains_volume(op_sim* s)
+{
+    const int G = s->p.ngrains;
+    const int T = omp_get_max_threads();
+    double* part = (double*)calloc((size_t)T*G, sizeof(double));
+    #pragma omp parallel
+    {
+        double* mine = part + (size_t)omp_get_thread_num()*G;
+        #pragma omp for schedule(static)
+        for (long v = 0; v < s->n; v++)
+        {
+            const entry* L = s->e + v*s->cap;
+            for (int a = 0; a < s->cnt[v]; a++) mine[L[a].idx] += L[a].val;
+        }
+    }
+    for (int g = 0; g < G; g++)
+    {
+        s->volume[g] = 0.0;
+        for (int t = 0; t < T; t++) s->volume[g] += part[(size_t)t*G + g];
+    }
+    free(part);
+    for (int g = 0; g < G; g++)
+    {
+        s->max_volume[g] = dmax(s->volume[g], s->max_volume[g]);
+        s->vr[g] = s->max_volume[g]/s->ref_volume[g];
+    }
+    for (int g = 0; g < G; g++)
+    {
+        if (s->exist[g] && s->volume[g] <= 0.0)
+        {
+            s->exist[g] = 0; s->stage[g] = OP_STAGE_STABLE;
+            s->volume[g] = 0.0; s->max_volume[g] = 0.0; s->vr[g] = 1.0;
+        }
+        else if (s->volume[g] > 0.0)
+        {
+            s->exist[g] = 1;
+            if (s->stage[g] == OP_STAGE_SEED) s->stage[g] = OP_STAGE_NUCLEUS;
+            if (s->vr[g] > 1.0) { s->stage[g] = OP_STAGE_STABLE; s->vr[g] = 1.0; }
+        }
+    }
+}
+
+/* PhaseField::FinalizeSR (src/PhaseField.cpp:1008-1033): node finalize on wide-interface voxels,
+ * then flags, derivatives and grain volumes (the periodic BoundaryConditions calls are implicit in
+ * the periodic neighbour indexing). */
+static void finalize_sr(op_sim* s)
+{
+    uint32_t st = 0;
+    #pragma omp parallel for schedule(static) reduction(|:st)
+    for (long v = 0; v < s->n; v++)
+    if (s->flag[v] != 0)
+    {
+        s->flag[v] = (int8_t)node_finalize(s->e + v*s->cap, &s->cnt[v], &st);
+    }
+    s->status |= st;
+    set_flags(s);
+    calculate_derivatives(s);
+    calculate_grains_volume(s);
+}
+
+void op_finalize_initialization(op_sim* s)
+{
+    finalize_sr(s);
+}
+
+uint32_t op_step(op_sim* s, double dt, int nsteps)
+{
+    const int cap = s->cap;
+    const int maxpairs = cap*(cap - 1)/2;
+    for (int t = 0; t < nsteps; t++)
+    {
+        uint32_t st = 0;
+        #pragma omp parallel reduction(|:st)
+        {
+            pair* P = (pair*)malloc(maxpairs*sizeof(pair));
+            #pragma omp for schedule(static)
+            for (long v = 0; v < s->n; v++)
+            {
+                if (s->flag[v] == 0) continue;
+                entry* L = s->e + v*cap;
+                const int n = s->cnt[v];
+                const int np = do_increments(s, L, n, P);
+                if (s->dg && s->flag[v] == 2) df_merge(s, L, n, P);
+                st |= normalize(L, n, P, np, dt);
+                merge(L, P, np, dt);
+            }
+            free(P);
+        }
+        s->status |= st;
+        finalize_sr(s);
+    }
+    const uint32_t r = s->status;
+    s->status = 0;
+    return r;
+}
+
+long op_total_entries(const op_sim* s)
+{
+    long t = 0;
+    for (long v = 0; v < s->n; v++) t += s->cnt[v];
+    return t;
+}
+
+void op_get_state(const op_sim* s, int32_t* counts, int32_t* idx, double* val)
+{
+    long off = 0;
+    for (long v = 0; v < s->n; v++)
+    {
+        counts[v] = s->cnt[v];
+        for (int a = 0; a < s->cnt[v]; a++)
+        {
+            idx[off] = s->e[v*s->cap + a].idx;
+            val[off] = s->e[v*s->cap + a].val;
+            off++;
+        }
+    }
+}
+
+void op_get_flags(const op_sim* s, int8_t* flags)
+{
+    memcpy(flags, s->flag, s->n);
+}
+
+long op_wide_count(const op_sim* s)
+{
+    long w = 0;
+    for (long v = 0; v < s->n; v++) w += (s->flag[v] != 0);
+    return w;
+}
+
+void op_get_grains(const op_sim* s, double* volume, double* volume_ratio, double* max_volume,
+                   int32_t* exist, int32_t* stage)
+{
+    const int G = s->p.ngrains;
+    if (volume) memcpy(volume, s->volume, G*sizeof(double));
+    if (volume_ratio) memcpy(volume_ratio, s->vr, G*sizeof(double));
+    if (max_volume) memcpy(max_volume, s->max_volume, G*sizeof(double));
+    if (exist) memcpy(exist, s->exist, G*sizeof(int32_t));
+    if (stage) memcpy(stage, s->stage, G*sizeof(int32_t));
+}
+
+void op_set_grains(op_sim* s, const double* volume_ratio, const double* max_volume,
+                   const int32_t* exist, const int32_t* stage, const double* ref_volume)
+{
+    const int G = s->p.ngrains;
+    if (volume_ratio) memcpy(s->vr, volume_ratio, G*sizeof(double));
+    if (max_volume) memcpy(s->max_volume, max_volume, G*sizeof(double));
+    if (exist) memcpy(s->exist, exist, G*sizeof(int32_t));
+    if (stage) memcpy(s->stage, stage, G*sizeof(int32_t));
+    if (ref_volume) memcpy(s->ref_volume, ref_volume, G*sizeof(double));
+}
