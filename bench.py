@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Throughput of the multiphase-field time step on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 256^3 periodic grain growth with driving force -- 2000 seeded Voronoi grains, eta = 6 dx,
+per-grain-pair sigma ~ U[0.8, 1.2], mu = 1, per-grain dG ~ U[0, 0.05], D3Q27 (LB) Laplacian,
+dt = 0.08 (synthetic, seeded; the grid does not fit any public dataset).  One "step" is one full
+time step of the grid.  `value` is voxel-updates/s of the FP32 form with the state resident in
+HBM; the FP64 form (the parity drop-in) is measured the same way and reported under "fp64".
+`e2e` is the same metric through the C ABI from pinned host buffers: upload of the initial state,
+per step the driving-force upload and the grain-volume download, and the final state download.
+
+Multi-GPU: every rank runs an independent replica of the workload (weak scaling); the timed region
+is bracketed by a barrier and the device time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "voxel-updates/s & HBM% peak: FP32 vs FP64 GPU at |Δφ|≤1e-4; adjoint/fwd ratio"
+UNIT = "voxel-updates/s"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(precision):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "step_kernel_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(precision)
+    except (ValueError, KeyError):
+        return None
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:  # noqa: BLE001 - clocks are reported as unavailable
+            self.ok = False
+
+    def _run(self):
+        nv = self._nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                self.reasons |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        names = [n for b, n in self.REASONS.items() if self.reasons & b and n != "gpu_idle"]
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": names, "samples": len(self.samples)}
+
+
+def build_inputs(case, threads=0):
+    t = time.time()
+    state = case.initial_state(threads)
+    sigma = case.pair_sigma()
+    dg = case.driving_force()
+    return state, sigma, dg, time.time() - t
+
+
+def device_run(case, precision, k_slots, steps, warmup, device, state, sigma, dg, dist):
+    """Device-resident throughput: W warm-up steps, then exactly K timed steps."""
+    import torch
+    from openphase_b200.context import Context
+
+    ctx = Context(case.nx, case.ny, case.nz, dx=case.dx, iwidth=case.iwidth, stencil=case.stencil,
+                  gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
+    ctx.set_model([[case.sigma]], [[case.mu]], limit=[[case.limit]], limiting=case.limiting,
+                  regularization=case.regularization)
+    ctx.set_grains(case.ngrains)
+    ctx.set_pair_table(sigma, None)
+    ctx.set_driving_force(dg)
+    ctx.upload(*state)
+    ctx.finalize_initialization()
+    ctx.step(case.dt, warmup)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    s0 = ctx.stats()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    ctx.set_timing(True)
+    with ClockSampler(device) as clk:
+        e0.record(stream)
+        ctx.step_async(case.dt, steps)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+    status = ctx.sync()
+    if dist is not None:
+        dist.barrier()
+    elapsed_ms = e0.elapsed_time(e1)
+    s1 = ctx.stats()
+    ctx.set_timing(False)
+    entries_in = s1["entries_in_total"] - s0["entries_in_total"]
+    entries_out = s1["entries_out_total"] - s0["entries_out_total"]
+    wide = s1["wide_total"] - s0["wide_total"]
+    ctx.close()
+    return {
+        "elapsed_ms": elapsed_ms, "kernel_ms": s1["timed_kernel_ms"], "kernel_launches": s1["timed_launches"],
+        "entries_in": entries_in, "entries_out": entries_out, "wide": wide, "status": status | s1["status"],
+        "clocks": clk.summary(),
+    }
+
+
+def e2e_run(case, precision, k_slots, steps, device, state, sigma, dg):
+    """End to end through the C ABI with pinned host buffers; host<->device copies inside the clock."""
+    import torch
+    from openphase_b200.context import Context
+
+    counts, idx, val = state
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_counts, h_idx, h_val, h_dg = pin(counts.astype(np.int32)), pin(idx.astype(np.int32)), pin(val), pin(dg)
+    h_vol = torch.empty(case.ngrains, dtype=torch.float64).pin_memory().numpy()
+    ctx = Context(case.nx, case.ny, case.nz, dx=case.dx, iwidth=case.iwidth, stencil=case.stencil,
+                  gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
+    ctx.set_model([[case.sigma]], [[case.mu]], limit=[[case.limit]], limiting=case.limiting,
+                  regularization=case.regularization)
+    ctx.set_grains(case.ngrains)
+    ctx.set_pair_table(sigma, None)
+    torch.cuda.synchronize(device)
+    from openphase_b200._lib import lib, ptr
+    L = lib()
+    t0 = time.perf_counter()
+    ctx.set_driving_force(h_dg)
+    ctx.upload(h_counts, h_idx, h_val)
+    ctx.finalize_initialization()
+    for _ in range(steps):
+        ctx.set_driving_force(h_dg)                       # the step's input: per-grain driving forces
+        ctx.step(case.dt, 1)
+        L.opgpu_grains(ctx.h, ptr(h_vol), None, None, None, None)   # the step's result: grain volumes
+    final = ctx.download()
+    t1 = time.perf_counter()
+    ctx.close()
+    h2d = h_counts.nbytes + h_idx.nbytes + h_val.nbytes + (steps + 1) * h_dg.nbytes
+    d2h = steps * h_vol.nbytes + final[0].nbytes + final[1].nbytes + final[2].nbytes
+    return {"seconds": t1 - t0, "h2d_per_step": h2d / steps, "d2h_per_step": d2h / steps}
+
+
+def reference_steps(case, state, warmup, steps, threads):
+    """Time the reference's own CPU implementation (oracle/_ref, built from the reference sources)
+    on the host cores: returns per-step seconds of the timed steps and the thread count."""
+    from oracle.bridge import reference_available, run_reference
+    if not reference_available():
+        return None
+    res, stats = run_reference(case.with_(nsteps=warmup + steps), *state, [warmup + steps], threads=threads)
+    per_step = stats["step_seconds"]
+    per_step = per_step if isinstance(per_step, list) else [per_step]
+    return per_step[warmup:warmup + steps], int(stats["threads"])
+
+
+def oracle_port_steps(case, state, warmup, steps, threads):
+    from oracle.bridge import Oracle
+    ora = Oracle(case, *state, cap=16, threads=threads)
+    ora.step(warmup)
+    out = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        ora.step(1)
+        out.append(time.perf_counter() - t)
+    return out, threads
+
+
+def cpu_baseline(case, state, threads, steps=2, warmup=1):
+    r = reference_steps(case, state, warmup, steps, threads)
+    kind = "reference"
+    if r is None:
+        r = oracle_port_steps(case, state, warmup, steps, threads)
+        kind = "port"
+    per_step, cores = r
+    value = case.n * len(per_step) / sum(per_step)
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{len(per_step)} timed full-grid steps after {warmup} warm-up step(s) of the same "
+                      f"{case.nx}^3 workload, OpenMP on {cores} host threads"}
+
+
+def run_reference_arm(args, case, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    state, sigma, dg, _ = build_inputs(case, threads)
+    # a bounded sample of the workload: full-grid reference steps, capped so the arm ends in minutes
+    warm = min(args.warmup, 1)
+    k = max(1, min(args.steps, 6))
+    r = reference_steps(case, state, warm, k, threads)
+    kind = "reference"
+    if r is None:
+        r = oracle_port_steps(case, state, warm, k, threads)
+        kind = "port"
+    per_step, cores = r
+    value = case.n * len(per_step) / sum(per_step)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": len(per_step), "warmup": warm, "ms_per_step": 1e3 * sum(per_step) / len(per_step),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{len(per_step)} full-grid steps after {warm} warm-up step(s), "
+                                   f"OpenMP on {cores} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--k-slots", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="grain_growth_dg_256")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    from openphase_b200 import cases
+    case = getattr(cases, args.workload)()
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        return run_reference_arm(args, case, rank)
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+
+    threads = max(1, (os.cpu_count() or 1) // max(1, world))
+    state, sigma, dg, t_init = build_inputs(case, threads)
+
+    runs = {}
+    for precision in ("fp32", "fp64"):
+        runs[precision] = device_run(case, precision, args.k_slots, args.steps, args.warmup, local_rank,
+                                     state, sigma, dg, dist)
+
+    def agg(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    out = {}
+    for precision, r in runs.items():
+        ms = agg(r["elapsed_ms"])
+        s = 4 if precision == "fp32" else 8
+        value = world * case.n * args.steps / (ms / 1e3)
+        launches = max(1, r["kernel_launches"])
+        kernel_ms = r["kernel_ms"] / launches
+        # algorithmic bytes of one step: every voxel's count byte and stored entries read once,
+        # the new count byte and entries written once
+        bytes_per_launch = 2 * case.n + (r["entries_in"] + r["entries_out"]) * (2 + s) / args.steps
+        achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
+        traffic = profiled_traffic(precision)
+        out[precision] = {
+            "value": value, "ms_per_step": ms / args.steps, "status": r["status"], "clocks": r["clocks"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "step_kernel", "kernel_ms": kernel_ms,
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s"},
+            "wide_fraction": r["wide"] / (case.n * args.steps),
+        }
+
+    e2e = None
+    if not args.no_e2e:
+        er = e2e_run(case, "fp32", args.k_slots, args.steps, local_rank, state, sigma, dg)
+        sec = agg(er["seconds"] * 1e3) / 1e3
+        e2e = {"value": world * case.n * args.steps / sec, "unit": UNIT,
+               "h2d_bytes_per_step": int(er["h2d_per_step"]), "d2h_bytes_per_step": int(er["d2h_per_step"])}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case, state, os.cpu_count() or 1)
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    f32, f64 = out["fp32"], out["fp64"]
+    line = {
+        "metric": METRIC, "value": f32["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": f32["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains,
+                   "eta_cells": case.iwidth, "dt": case.dt, "stencil": "D3Q27 (LB)", "k_slots": args.k_slots,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (the K-slot state is >126 MB)",
+                   "initial_state_seconds": round(t_init, 2)},
+        "clocks": f32["clocks"],
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "roofline": f32["roofline"],
+        "cpu_baseline": cpu,
+        "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "roofline": f64["roofline"],
+                 "clocks": f64["clocks"], "status": f64["status"]},
+        "fp32_over_fp64": f32["value"] / f64["value"],
+        "status": {"fp32": f32["status"], "fp64": f64["status"]},
+        "wide_fraction": f32["wide_fraction"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

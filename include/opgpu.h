@@ -86,6 +86,8 @@ typedef struct opgpu_stats {
     int64_t entries_out_total;     /* sum over steps of stored entries written                    */
     uint32_t status;               /* OR of soft OPGPU_E_* bits since the last opgpu_clear_status  */
     uint32_t overflow_voxels;      /* voxels that raised OPGPU_E_OVERFLOW_K / _LIST               */
+    int64_t timed_launches;        /* step-kernel launches timed since opgpu_set_timing(ctx, 1)     */
+    double  timed_kernel_ms;       /* their summed device duration (CUDA events around each launch) */
 } opgpu_stats;
 
 /* ---- lifecycle ------------------------------------------------------------------------------ */
@@ -154,6 +156,10 @@ uint32_t opgpu_sync(opgpu_ctx* ctx);
 uint32_t opgpu_grains(opgpu_ctx* ctx, double* volume, double* volume_ratio, double* max_volume,
                       int32_t* exist, int32_t* stage);
 uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats);
+/* Time every fused step-kernel launch with a pair of CUDA events on the context's stream
+ * (enable = 1 resets the accumulated figures; 0 stops timing).  No reference counterpart: the
+ * reference's TimeInfo stamps (include/Tools/TimeInfo.h:36-86) are host wall-clock only. */
+uint32_t opgpu_set_timing(opgpu_ctx* ctx, int32_t enable);
 uint32_t opgpu_clear_status(opgpu_ctx* ctx);
 /* CUDA stream of the context (a cudaStream_t), for callers that order their own work after it. */
 void*    opgpu_stream(opgpu_ctx* ctx);
@@ -174,6 +180,13 @@ uint32_t opgpu_voronoi_owner_host(int32_t nx, int32_t ny, int32_t nz, int32_t ng
  * total; then with idx sized total. */
 uint32_t opgpu_spread_boundaries_host(int32_t nx, int32_t ny, int32_t nz, const int32_t* owner,
                                       int32_t threads, int32_t* counts, int32_t* idx, int64_t* total);
+
+/* Symmetric per-grain-pair table out[a*G+b] = lo + span*u(seed, stream, min(a,b), max(a,b)) with
+ * out[a*G+a] = lo; the table opgpu_set_pair_table takes (stream 2 for interface energies). */
+uint32_t opgpu_pair_table_host(int32_t ngrains, uint64_t seed, uint64_t stream, double lo, double span,
+                               double* out);
+/* Per-grain values out[g] = scale*u(seed, stream, g, 0) (stream 3 for driving forces). */
+uint32_t opgpu_grain_values_host(int32_t ngrains, uint64_t seed, uint64_t stream, double scale, double* out);
 
 #ifdef __cplusplus
 }

@@ -63,7 +63,8 @@ class Model(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("steps", C.c_int64), ("wide_last", C.c_int64), ("wide_total", C.c_int64),
                 ("entries_in_total", C.c_int64), ("entries_out_total", C.c_int64),
-                ("status", C.c_uint32), ("overflow_voxels", C.c_uint32)]
+                ("status", C.c_uint32), ("overflow_voxels", C.c_uint32), ("timed_launches", C.c_int64),
+                ("timed_kernel_ms", C.c_double)]
 
 
 _lib = None
@@ -94,12 +95,15 @@ _SIGS = {
     "opgpu_grains": (C.c_uint32, [_P, _P, _P, _P, _P, _P]),
     "opgpu_get_stats": (C.c_uint32, [_P, C.POINTER(Stats)]),
     "opgpu_clear_status": (C.c_uint32, [_P]),
+    "opgpu_set_timing": (C.c_uint32, [_P, C.c_int32]),
     "opgpu_stream": (_P, [_P]),
     "opgpu_uniform": (C.c_double, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
     "opgpu_voronoi_owner_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                               C.c_int32, _P]),
     "opgpu_spread_boundaries_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32, _P, _P,
                                                   C.POINTER(C.c_int64)]),
+    "opgpu_pair_table_host": (C.c_uint32, [C.c_int32, C.c_uint64, C.c_uint64, C.c_double, C.c_double, _P]),
+    "opgpu_grain_values_host": (C.c_uint32, [C.c_int32, C.c_uint64, C.c_uint64, C.c_double, _P]),
 }
 
 

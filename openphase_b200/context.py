@@ -138,6 +138,9 @@ class Context:
         _check(lib().opgpu_get_stats(self.h, C.byref(s)), self.h, "get_stats")
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
+    def set_timing(self, enable: bool):
+        _check(lib().opgpu_set_timing(self.h, int(enable)), self.h, "set_timing")
+
     def clear_status(self):
         _check(lib().opgpu_clear_status(self.h), self.h, "clear_status")
 

@@ -157,6 +157,33 @@ extern "C" uint32_t opgpu_spread_boundaries_host(int32_t nx, int32_t ny, int32_t
     return OPGPU_OK;
 }
 
+extern "C" uint32_t opgpu_pair_table_host(int32_t ngrains, uint64_t seed, uint64_t stream, double lo,
+                                          double span, double* out)
+{
+    if (ngrains <= 0 || !out) return OPGPU_E_INVALID;
+    const long G = ngrains;
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (long a = 0; a < G; a++)
+    {
+        out[a * G + a] = lo;
+        for (long b = a + 1; b < G; b++)
+        {
+            const double v = lo + span * opgpu::uniform01(seed, stream, (uint64_t)a, (uint64_t)b);
+            out[a * G + b] = v;
+            out[b * G + a] = v;
+        }
+    }
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_grain_values_host(int32_t ngrains, uint64_t seed, uint64_t stream, double scale,
+                                            double* out)
+{
+    if (ngrains <= 0 || !out) return OPGPU_E_INVALID;
+    for (int g = 0; g < ngrains; g++) out[g] = scale * opgpu::uniform01(seed, stream, (uint64_t)g, 0);
+    return OPGPU_OK;
+}
+
 namespace opgpu {
 
 // Raw PhaseField format (src/PhaseField.cpp:2340-2388, NodePF::write NodePF.h:765-775):

@@ -42,6 +42,12 @@ struct opgpu_ctx {
     bool model_set = false, state_loaded = false, initialized = false;
     uint32_t status = 0;
     double nvf = 1.0;   // NucleusVolumeFactor
+    // per-launch timing of the step kernel
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;          // event pairs recorded and not yet read
+    long long timed_launches = 0;
+    double timed_ms = 0.0;
 };
 
 namespace {
@@ -294,6 +300,14 @@ uint32_t read_status(opgpu_ctx* ctx)
     CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < ctx->ev_used; i++)
+    {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * i], ctx->ev_pool[2 * i + 1]));
+        ctx->timed_ms += ms;
+        ctx->timed_launches++;
+    }
+    ctx->ev_used = 0;
     ctx->status |= st;
     return st;
 }
@@ -378,6 +392,7 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int b = 0; b < 2; b++) { dfree(ctx->cnt[b]); dfree(ctx->idx[b]); dfree(ctx->val[b]); }
     free_grains(ctx);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -608,9 +623,27 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
         a.vr = ctx->d_vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
         a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
+        if (ctx->timing)
+        {
+            if (ctx->ev_pool.size() < 2 * (ctx->ev_used + 1))
+            {
+                for (int k = 0; k < 2; k++)
+                {
+                    cudaEvent_t e;
+                    CK(cudaEventCreate(&e));
+                    ctx->ev_pool.push_back(e);
+                }
+            }
+            CK(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], ctx->stream));
+        }
         const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->stream)
                                  : launch_step_f64(sp, a, ctx->K, ctx->stream);
         if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("step launch: ") + cudaGetErrorString((cudaError_t)rc));
+        if (ctx->timing)
+        {
+            CK(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used + 1], ctx->stream));
+            ctx->ev_used++;
+        }
         grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
             ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 1);
         CK(cudaGetLastError());
@@ -769,6 +802,21 @@ extern "C" uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats)
     stats->entries_out_total = (int64_t)c[kCntEntriesOutTotal];
     stats->status = ctx->status;
     stats->overflow_voxels = (uint32_t)c[kCntOverflowVoxels];
+    stats->timed_launches = ctx->timed_launches;
+    stats->timed_kernel_ms = ctx->timed_ms;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_timing(opgpu_ctx* ctx, int32_t enable)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    read_status(ctx);
+    ctx->timing = enable != 0;
+    if (enable)
+    {
+        ctx->timed_launches = 0;
+        ctx->timed_ms = 0.0;
+    }
     return OPGPU_OK;
 }
 

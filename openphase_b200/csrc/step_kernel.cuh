@@ -190,7 +190,9 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
 
             // ---- 2. double-obstacle pair kinetics -------------------------------------------
             constexpr int KP = KL * (KL - 1) / 2;
-            R pv[KP];
+            // pair increments are kept in FP64 from here on (the FP32 form widens the kinetics'
+            // result so that the projection's sums and limiter run as in the FP64 form)
+            double pv[KP];
             R sg[KP];
             R mg[KP];
             double localN;
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                     }
                 }
                 dphi *= mg[q] * norm_1 * scale;
-                pv[q] = dphi;
+                pv[q] = (double)dphi;
             }
 
             // ---- 3. driving force (interface voxels only) -----------------------------------
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                         locdG = allowed * tanh(locdG / allowed);
                     }
                     const double dpsi = locdG * (double)mg[q] * norm * p.pref_df;
-                    pv[q] = (R)((double)pv[q] + dpsi);
+                    pv[q] += dpsi;
                 }
             }
 
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                 const double old_value = (double)val[0];
                 if ((old_value == 0.0 && valueA < 0.0) || (old_value == 1.0 && valueA > 0.0))
                 {
-                    pv[0] = R(0);
+                    pv[0] = 0.0;
                 }
                 else
                 {
@@ -281,8 +283,8 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                     double norm = 1.0;
                     if (new_value < 0.0) norm *= -old_value / valueA;
                     else if (new_value > 1.0) norm *= (1.0 - old_value) / valueA;
-                    if (norm > DBL_EPSILON) pv[0] = (R)((double)pv[0] * norm);
-                    else pv[0] = R(0);
+                    if (norm > DBL_EPSILON) pv[0] *= norm;
+                    else pv[0] = 0.0;
                 }
             }
             else if (np > 1)
@@ -300,12 +302,12 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                         for (int j = 0; j < n; j++)
                         {
                             if (j == i) continue;
-                            pv[i < j ? pair_pos(i, j, n) : pair_pos(j, i, n)] = R(0);
+                            pv[i < j ? pair_pos(i, j, n) : pair_pos(j, i, n)] = 0.0;
                         }
                     }
                 }
                 bool any = false;
-                for (int q = 0; q < np; q++) any |= (pv[q] != R(0));
+                for (int q = 0; q < np; q++) any |= (pv[q] != 0.0);
                 if (any)
                 {
                     double pos[KL], neg[KL], limP[KL], limN[KL];
@@ -336,16 +338,16 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                         for (int j = i + 1; j < n; j++)
                         {
                             const int q = pair_pos(i, j, n);
-                            if (pv[q] < R(0))
+                            if (pv[q] < 0.0)
                             {
                                 const double lim = dmin_ref(limN[i], limP[j]);
-                                pv[q] = (R)((double)pv[q] * lim);
+                                pv[q] *= lim;
                                 if (lim < 1.0) needed = true;
                             }
-                            if (pv[q] > R(0))
+                            if (pv[q] > 0.0)
                             {
                                 const double lim = dmin_ref(limP[i], limN[j]);
-                                pv[q] = (R)((double)pv[q] * lim);
+                                pv[q] *= lim;
                                 if (lim < 1.0) needed = true;
                             }
                         }
@@ -356,7 +358,7 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                         }
                     }
                     for (int q = 0; q < np; q++)
-                        if (fabs((double)pv[q] * dt) < DBL_EPSILON) pv[q] = R(0);
+                        if (fabs(pv[q] * dt) < DBL_EPSILON) pv[q] = 0.0;
                     // plausibility check (a warning in the reference)
                     for (int i = 0; i < n; i++) pos[i] = (double)val[i];
                     for (int i = 0; i < n; i++)
@@ -371,16 +373,15 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
             }
 
             // ---- 5. merge (volume conserving, pair by pair) ---------------------------------
-            const R rdt = (R)dt;
             for (int i = 0; i < n; i++)
             for (int j = i + 1; j < n; j++)
             {
-                const R w = pv[pair_pos(i, j, n)];
-                const R value = R(1) * (w + R(0)) * rdt;
-                if (fabs((double)value) >= DBL_EPSILON)
+                const double w = pv[pair_pos(i, j, n)];
+                const double value = 1.0 * (w + 0.0) * dt;
+                if (fabs(value) >= DBL_EPSILON)
                 {
-                    val[i] += value;
-                    val[j] += -value;
+                    val[i] += (R)value;
+                    val[j] += (R)(-value);
                 }
             }
 

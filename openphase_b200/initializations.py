@@ -57,19 +57,20 @@ def voronoi(nx: int, ny: int, nz: int, ngrains: int, seed: int, threads: int = 0
 
 def sigma_table(ngrains: int, seed: int, lo: float = 0.8, span: float = 0.4) -> np.ndarray:
     """Symmetric G x G table sigma(a,b) = lo + span*u(seed, SIGMA, min, max); diagonal = lo."""
-    G = ngrains
-    t = np.empty((G, G), dtype=np.float64)
-    f = lib().opgpu_uniform
-    for a in range(G):
-        t[a, a] = lo
-        for b in range(a + 1, G):
-            t[a, b] = t[b, a] = lo + span * f(seed, STREAM_SIGMA, a, b)
+    t = np.empty((ngrains, ngrains), dtype=np.float64)
+    rc = lib().opgpu_pair_table_host(ngrains, seed, STREAM_SIGMA, lo, span, ptr(t))
+    if rc:
+        raise OpgpuError(rc, "pair_table_host")
     return t
 
 
 def driving_forces(ngrains: int, seed: int, scale: float) -> np.ndarray:
-    f = lib().opgpu_uniform
-    return np.array([scale * f(seed, STREAM_DRIVING_FORCE, g, 0) for g in range(ngrains)], dtype=np.float64)
+    """Per-grain stored-energy driving forces scale*u(seed, DRIVING_FORCE, g, 0)."""
+    d = np.empty(ngrains, dtype=np.float64)
+    rc = lib().opgpu_grain_values_host(ngrains, seed, STREAM_DRIVING_FORCE, scale, ptr(d))
+    if rc:
+        raise OpgpuError(rc, "grain_values_host")
+    return d
 
 
 def raw_bytes(nx: int, ny: int, nz: int, counts, idx, val) -> bytes:

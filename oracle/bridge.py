@@ -125,7 +125,10 @@ class Oracle:
     def step(self, nsteps, dt=None):
         return int(oracle_lib().op_step(self.h, self.case.dt if dt is None else dt, nsteps))
 
-    def state(self):
+    def state(self, positive_only=False):
+        """Per-voxel lists (counts, idx, val).  Like the reference's Fields after Finalize they include
+        the zero-valued candidate entries of CalculateDerivativesSR; positive_only drops them, which
+        leaves exactly the stored fields of the CUDA path."""
         L = oracle_lib()
         n = self.case.n
         total = L.op_total_entries(self.h)
@@ -133,6 +136,8 @@ class Oracle:
         idx = np.empty(total, dtype=np.int32)
         val = np.empty(total, dtype=np.float64)
         L.op_get_state(self.h, _p(counts), _p(idx), _p(val))
+        if positive_only:
+            return positive_entries(counts, idx, val)
         return counts, idx, val
 
     def flags(self):
@@ -149,6 +154,14 @@ class Oracle:
         ex, st = np.empty(G, dtype=np.int32), np.empty(G, dtype=np.int32)
         oracle_lib().op_get_grains(self.h, _p(vol), _p(vr), _p(mx), _p(ex), _p(st))
         return {"volume": vol, "volume_ratio": vr, "max_volume": mx, "exist": ex, "stage": st}
+
+
+def positive_entries(counts, idx, val):
+    """Drop zero-valued entries from ragged lists, keeping the order of the rest."""
+    keep = np.asarray(val) != 0.0
+    vox = np.repeat(np.arange(counts.size), counts)
+    new_counts = np.bincount(vox[keep], minlength=counts.size).astype(np.int32)
+    return new_counts, np.asarray(idx)[keep], np.asarray(val)[keep]
 
 
 def reference_available() -> bool:

@@ -246,6 +246,7 @@ int main(int argc, char* argv[])
     const size_t G = c.ngrains;
 
     std::vector<long> wide(c.nsteps + 1, 0);
+    std::vector<double> step_seconds(c.nsteps + 1, 0.0);
     double t_loop = 0.0;
     for (int step = 1; step <= c.nsteps; step++)
     {
@@ -297,7 +298,8 @@ int main(int argc, char* argv[])
         }
         Phi.NormalizeIncrements(BC, c.dt);
         Phi.MergeIncrements(BC, c.dt);
-        t_loop += omp_get_wtime() - t0;
+        step_seconds[step] = omp_get_wtime() - t0;
+        t_loop += step_seconds[step];
 
         long w = 0;
         #pragma omp parallel for collapse(3) reduction(+:w)
@@ -318,6 +320,9 @@ int main(int argc, char* argv[])
     st << "nsteps " << c.nsteps << "\n";
     st << "wide";
     for (int s = 1; s <= c.nsteps; s++) st << " " << wide[s];
+    st << "\n";
+    st << "step_seconds";
+    for (int s = 1; s <= c.nsteps; s++) st << " " << step_seconds[s];
     st << "\n";
     return 0;
 }

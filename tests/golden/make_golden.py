@@ -1,0 +1,55 @@
+"""Generate the golden fixtures of the phase-field step from the unmodified reference.
+
+Runs the reference (compiled from its own sources by `make -C oracle ref`, driven through its public
+API by oracle/ref_driver.cpp) on small seeded cases and stores, per case, the states and grain
+records at a few checkpoints.  The fixtures pin the oracle (tests/test_oracle.py) without needing the
+reference at test time.
+
+    python tests/golden/make_golden.py            # writes tests/golden/*.npz
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+from openphase_b200.cases import Case  # noqa: E402
+from oracle.bridge import run_reference  # noqa: E402
+
+GOLDEN_CASES = {
+    "lb_16": (Case(16, 16, 16, 6, seed=3, iwidth=4.0, dt=0.1, name="lb_16"), [1, 10, 50]),
+    "isotropic_24x20x16": (Case(24, 20, 16, 10, seed=5, iwidth=5.0, dt=0.1, stencil="ISOTROPIC",
+                                name="isotropic_24x20x16"), [1, 40]),
+    "simple_24x20x16": (Case(24, 20, 16, 10, seed=5, iwidth=5.0, dt=0.1, stencil="SIMPLE",
+                             name="simple_24x20x16"), [1, 40]),
+    "pairs_dg_24": (Case(24, 24, 24, 30, seed=7, iwidth=6.0, dt=0.08, sigma=1.2, sigma_pairs=(0.8, 0.4),
+                         dg_scale=0.05, name="pairs_dg_24"), [1, 60]),
+    "dg_strong_20": (Case(20, 20, 20, 40, seed=9, iwidth=4.0, dt=0.1, sigma=1.2, sigma_pairs=(0.8, 0.4),
+                          dg_scale=0.3, name="dg_strong_20"), [1, 60]),
+}
+
+
+def main():
+    for name, (case, steps) in GOLDEN_CASES.items():
+        counts, idx, val = case.initial_state()
+        res, stats = run_reference(case, counts, idx, val, [0] + steps, threads=4)
+        arrays = {"init_counts": counts.astype(np.uint8), "init_idx": idx.astype(np.int16)}
+        for s in [0] + steps:
+            c, i, v, vol, vr = res[s]
+            arrays[f"s{s}_counts"] = c.astype(np.uint8)
+            arrays[f"s{s}_idx"] = i.astype(np.int16)
+            arrays[f"s{s}_val"] = v
+            arrays[f"s{s}_volume"] = vol
+            arrays[f"s{s}_volume_ratio"] = vr
+        arrays["wide"] = np.asarray(stats["wide"] if isinstance(stats["wide"], list) else [stats["wide"]],
+                                    dtype=np.int64)
+        np.savez_compressed(HERE / f"{name}.npz", **arrays)
+        print(name, {k: v.shape for k, v in arrays.items() if k.endswith("_val")})
+
+
+if __name__ == "__main__":
+    main()
