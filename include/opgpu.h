@@ -156,6 +156,9 @@ uint32_t opgpu_sync(opgpu_ctx* ctx);
 uint32_t opgpu_grains(opgpu_ctx* ctx, double* volume, double* volume_ratio, double* max_volume,
                       int32_t* exist, int32_t* stage);
 uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats);
+/* Kernel variant of opgpu_step: 0 = tiled production kernel (default), 1 = full-grid generic
+ * kernel with identical arithmetic (kept for validation).  No reference counterpart. */
+uint32_t opgpu_set_kernel_variant(opgpu_ctx* ctx, int32_t variant);
 /* Time every fused step-kernel launch with a pair of CUDA events on the context's stream
  * (enable = 1 resets the accumulated figures; 0 stops timing).  No reference counterpart: the
  * reference's TimeInfo stamps (include/Tools/TimeInfo.h:36-86) are host wall-clock only. */

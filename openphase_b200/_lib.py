@@ -96,6 +96,7 @@ _SIGS = {
     "opgpu_get_stats": (C.c_uint32, [_P, C.POINTER(Stats)]),
     "opgpu_clear_status": (C.c_uint32, [_P]),
     "opgpu_set_timing": (C.c_uint32, [_P, C.c_int32]),
+    "opgpu_set_kernel_variant": (C.c_uint32, [_P, C.c_int32]),
     "opgpu_stream": (_P, [_P]),
     "opgpu_uniform": (C.c_double, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
     "opgpu_voronoi_owner_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,

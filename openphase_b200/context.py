@@ -138,6 +138,11 @@ class Context:
         _check(lib().opgpu_get_stats(self.h, C.byref(s)), self.h, "get_stats")
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
+    def set_kernel_variant(self, variant: str):
+        """'tiled' (production) or 'generic' (full-grid kernel, same arithmetic)."""
+        code = {"tiled": 0, "generic": 1}[variant]
+        _check(lib().opgpu_set_kernel_variant(self.h, code), self.h, "set_kernel_variant")
+
     def set_timing(self, enable: bool):
         _check(lib().opgpu_set_timing(self.h, int(enable)), self.h, "set_timing")
 

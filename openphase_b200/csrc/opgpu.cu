@@ -38,6 +38,9 @@ struct opgpu_ctx {
     double *d_dg = nullptr, *d_pair_sigma = nullptr, *d_pair_mu = nullptr;
     uint32_t* d_status = nullptr;
     unsigned long long* d_counters = nullptr;
+    int* d_slow_list = nullptr;      // overflow worklist of the tiled kernel (capacity N)
+    unsigned* d_slow_count = nullptr;
+    int variant = kVariantTiled;
     StepParams sp{};
     bool model_set = false, state_loaded = false, initialized = false;
     uint32_t status = 0;
@@ -367,6 +370,8 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
         if (cudaMalloc(&ctx->val[b], (size_t)ctx->n * ctx->K * ctx->rsz + 16) != cudaSuccess) return bail(OPGPU_E_CUDA);
         if (cudaMemset(ctx->cnt[b], 0, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
     }
+    if (dalloc(&ctx->d_slow_list, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    if (dalloc(&ctx->d_slow_count, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
     if (dalloc(&ctx->d_status, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
     if (dalloc(&ctx->d_counters, kNumCounters) != cudaSuccess) return bail(OPGPU_E_CUDA);
     cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
@@ -377,7 +382,9 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
     const double Eta = g.iwidth * g.dx;                 // src/GridParameters.cpp:256
     sp.pref_do = kPi * kPi / (Eta * Eta);               // src/DoubleObstacle.cpp:504
     sp.pref_df = kPi / Eta;                             // src/DrivingForce.cpp:507
-    sp.eps_snap = ctx->fp32 ? (double)FLT_EPSILON : DBL_EPSILON;
+    // finalize snaps at DBL_EPSILON in both forms: the FP32 form merges and finalizes in FP64 and
+    // rounds only the stored values, so its erase decisions follow the FP64 form's
+    sp.eps_snap = DBL_EPSILON;
     sp.consider_nucleus_volume = 1;
     sp.limiting = 1;
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(OPGPU_E_CUDA);
@@ -393,6 +400,8 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     for (int b = 0; b < 2; b++) { dfree(ctx->cnt[b]); dfree(ctx->idx[b]); dfree(ctx->val[b]); }
     free_grains(ctx);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    dfree(ctx->d_slow_list);
+    dfree(ctx->d_slow_count);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -623,6 +632,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
         a.vr = ctx->d_vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
         a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
+        a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
         if (ctx->timing)
         {
             if (ctx->ev_pool.size() < 2 * (ctx->ev_used + 1))
@@ -636,8 +646,8 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
             }
             CK(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], ctx->stream));
         }
-        const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->stream)
-                                 : launch_step_f64(sp, a, ctx->K, ctx->stream);
+        const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->variant, ctx->stream)
+                                 : launch_step_f64(sp, a, ctx->K, ctx->variant, ctx->stream);
         if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("step launch: ") + cudaGetErrorString((cudaError_t)rc));
         if (ctx->timing)
         {
@@ -804,6 +814,15 @@ extern "C" uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats)
     stats->overflow_voxels = (uint32_t)c[kCntOverflowVoxels];
     stats->timed_launches = ctx->timed_launches;
     stats->timed_kernel_ms = ctx->timed_ms;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_kernel_variant(opgpu_ctx* ctx, int32_t variant)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    if (variant != kVariantTiled && variant != kVariantGeneric)
+        return fail(ctx, OPGPU_E_INVALID, "opgpu_set_kernel_variant: 0 (tiled) or 1 (generic)");
+    ctx->variant = variant;
     return OPGPU_OK;
 }
 

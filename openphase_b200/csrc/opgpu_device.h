@@ -77,10 +77,17 @@ struct StepArrays {
     double* vol_acc;           // [G] volume accumulator of the output state (zeroed by the caller)
     uint32_t* status;          // soft status bits
     unsigned long long* counters;  // kNumCounters
+    // overflow worklist of the tiled kernel (voxels whose lists exceed its register capacity)
+    int* slow_list;            // [slow_cap]
+    unsigned* slow_count;      // reset by the launcher before every step
+    unsigned slow_cap;
 };
 
-// Launchers (defined in step_f64.cu / step_f32.cu).  k_slots in {8, 12, 16}.
-int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
-int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
+enum { kVariantTiled = 0, kVariantGeneric = 1 };
+
+// Launchers (defined in step_f64.cu / step_f32.cu).  k_slots in {8, 12, 16}; variant selects the
+// tiled production kernel or the full-grid generic kernel (same results, used for validation).
+int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream);
+int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream);
 
 }  // namespace opgpu

@@ -1,10 +1,10 @@
 // FP32 form of the fused step: field values, increments and stencil arithmetic in FP32; the
 // simplex sums (limiter sums, finalize total) and the grain-volume reduction stay in FP64.
-#include "step_kernel.cuh"
+#include "tile_kernel.cuh"
 
 namespace opgpu {
-int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, void* stream)
+int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream)
 {
-    return launch_step<float>(p, a, k_slots, stream);
+    return launch_step<float>(p, a, k_slots, variant, stream);
 }
 }  // namespace opgpu

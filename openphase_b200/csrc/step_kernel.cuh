@@ -70,22 +70,16 @@ __device__ __forceinline__ void vol_insert(int* keys, double* sums, double* glob
     atomicAdd(&global_acc[g], v);
 }
 
+// One voxel of the step, reading its 3x3x3 neighbourhood straight from global memory, with the
+// field+candidate list and the pair increments in local memory (capacity KL entries).  This is
+// the general path: the full-grid reference kernel below and the overflow kernel of the tiled step
+// (voxels whose lists exceed the tiled kernel's register capacity) both run it.
 template <class R, int KS, int KL>
-__global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepParams p, const StepArrays a)
+__device__ __forceinline__ void voxel_step_generic(const StepParams& p, const StepArrays& a, long long v,
+                                                   int* s_key, double* s_sum, unsigned& wide, unsigned& ein,
+                                                   unsigned& eout, uint32_t& st, bool count_in)
 {
-    __shared__ int s_key[kVolSlots];
-    __shared__ double s_sum[kVolSlots];
-    __shared__ unsigned long long s_cnt[3];
-    for (int i = threadIdx.x; i < kVolSlots; i += blockDim.x) { s_key[i] = -1; s_sum[i] = 0.0; }
-    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0ull;
-    __syncthreads();
-
     const long long N = p.n;
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned wide = 0, ein = 0, eout = 0;
-    uint32_t st = 0;
-
-    if (v < N)
     {
         const uint8_t* __restrict__ cnt = a.cnt_in;
         const int16_t* __restrict__ gin = a.idx_in;
@@ -373,6 +367,9 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
             }
 
             // ---- 5. merge (volume conserving, pair by pair) ---------------------------------
+            // accumulated in FP64; the FP32 form rounds only when the record is stored
+            double vd[KL];
+            for (int i = 0; i < n; i++) vd[i] = (double)val[i];
             for (int i = 0; i < n; i++)
             for (int j = i + 1; j < n; j++)
             {
@@ -380,29 +377,29 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
                 const double value = 1.0 * (w + 0.0) * dt;
                 if (fabs(value) >= DBL_EPSILON)
                 {
-                    val[i] += (R)value;
-                    val[j] += (R)(-value);
+                    vd[i] += value;
+                    vd[j] += -value;
                 }
             }
 
             // ---- 6. finalize: snap, erase, renormalise --------------------------------------
             double total = 0.0;
             int m = 0;
-            const R hi_snap = (R)(1.0 - p.eps_snap);
-            const R lo_snap = (R)(0.0 + p.eps_snap);
+            const double hi_snap = 1.0 - p.eps_snap;
+            const double lo_snap = 0.0 + p.eps_snap;
             for (int i = 0; i < n; i++)
             {
-                R w = val[i];
+                double w = vd[i];
                 bool erase = false;
-                if (w >= hi_snap) w = R(1);
-                if (w <= lo_snap) { w = R(0); erase = true; }
-                total += (double)w;
-                if (!erase) { gL[m] = gL[i]; val[m] = w; m++; }
+                if (w >= hi_snap) w = 1.0;
+                if (w <= lo_snap) { w = 0.0; erase = true; }
+                total += w;
+                if (!erase) { gL[m] = gL[i]; vd[m] = w; m++; }
             }
             if (m > 1)
             {
                 const double norm = 1.0 / total;
-                for (int i = 0; i < m; i++) val[i] = (R)((double)val[i] * norm);
+                for (int i = 0; i < m; i++) val[i] = (R)(vd[i] * norm);
             }
             else if (m == 1)
             {
@@ -424,6 +421,23 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
             eout = m;
         }
     }
+    if (!count_in) { ein = 0; }
+}
+
+template <class R, int KS, int KL>
+__global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepParams p, const StepArrays a)
+{
+    __shared__ int s_key[kVolSlots];
+    __shared__ double s_sum[kVolSlots];
+    __shared__ unsigned long long s_cnt[3];
+    for (int i = threadIdx.x; i < kVolSlots; i += blockDim.x) { s_key[i] = -1; s_sum[i] = 0.0; }
+    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned wide = 0, ein = 0, eout = 0;
+    uint32_t st = 0;
+    if (v < p.n) voxel_step_generic<R, KS, KL>(p, a, v, s_key, s_sum, wide, ein, eout, st, true);
 
     if (st) atomicOr(a.status, st);
     // block totals of the counters
@@ -450,7 +464,7 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
 }
 
 template <class R>
-int launch_step(const StepParams& p, const StepArrays& a, int k_slots, void* stream)
+int launch_step_generic(const StepParams& p, const StepArrays& a, int k_slots, void* stream)
 {
     const int threads = 256;
     const long long blocks = (p.n + threads - 1) / threads;

@@ -35,8 +35,7 @@ def test_fp32_error_against_fp64_oracle(case):
         ora.step(s - prev)
         prev = s
         assert st & 0b11 == 0
-        r = compare_states(f32.download(), ora.state(positive_only=True), case.ngrains,
-                           eps_snap=float(np.finfo(np.float32).eps))
+        r = compare_states(f32.download(), ora.state(positive_only=True), case.ngrains)
         g32, g64 = f32.grains()["volume"], ora.grains()["volume"]
         live = g64 > 100.0
         vol_err = float(np.max(np.abs(g32[live] - g64[live]) / g64[live]))
