@@ -1,60 +1,70 @@
 // Tiled form of the fused step (the production path).
 //
 // A block owns a (y, z) tile of TY x 32 voxels and marches along x over `xchunk` planes.  The 3x3x3
-// neighbourhoods come from a ring of three x-planes held in shared memory (tile plus a one-voxel
-// halo in y and z, periodic wrap by index arithmetic); only the first KT stored slots of a record
-// are staged, the rare deeper slots are read from global memory.  Every plane goes through
-//
-//   A  (thread per voxel)   flag from the 27 neighbour counts; bulk voxels are copied straight to
-//                           the output; interface voxels build their field + candidate list with
-//                           Laplacians in registers (capacity NF) and park it in shared memory.
-//                           Lists longer than NF go to the overflow worklist (generic kernel).
-//   B  (thread per list)    lists are bucketed by length so that each warp runs one
-//                           length-specialised, fully unrolled path for the pair kinetics,
-//                           driving force, projection, merge and finalize (registers only).
-//   C  (thread per voxel)   the new records are written back coalesced and the grain volumes
-//                           are accumulated in a per-block shared-memory table.
+// neighbourhoods come from a ring of three x-planes in shared memory (tile plus a one-voxel halo in
+// y and z; periodic wrap by index arithmetic).  The grains present in the three planes of the
+// window get block-local slot numbers (at most kSlots, recycled as grains leave the window), and
+// every ring plane is held twice:
+//   * as per-record slot lists in the record's entry order plus a slot bitmask, and
+//   * as dense per-slot value planes dense[slot][plane][record] (zero where the grain is absent).
+// Every plane then goes through
+//   A  (thread per voxel)  flag from the 27 neighbour counts; bulk voxels are copied straight to
+//                          the output; interface voxels discover their candidate fields with
+//                          bitmask operations, in the reference's order (own fields, then new
+//                          grains in stencil order and neighbour-list order).
+//   B  (thread per list)   lists are bucketed by length; each warp runs one length-specialised,
+//                          fully unrolled path: Laplacians from the dense planes (27 loads and
+//                          multiply-adds per field), pair kinetics, driving force, projection,
+//                          merge and finalize, all in registers.
+//   C  (thread per voxel)  the new records are written back coalesced; grain volumes accumulate in
+//                          a per-block shared-memory table.
+// Lists longer than NF and windows with more than kSlots distinct grains go to the overflow
+// worklist, which the general per-voxel kernel processes afterwards.
 //
 // The per-voxel arithmetic and its operation order are those of voxel_step_generic (and of the
-// reference), so both kernels give bit-identical FP64 results.
+// reference: a Laplacian sums w*phi over the stencil in stencil order; adding the zero terms of
+// absent neighbours leaves every partial sum unchanged), so the FP64 results agree bit for bit.
 #pragma once
 #include "step_kernel.cuh"
 
 namespace opgpu {
 
 constexpr int kTileZ = 32;
+constexpr int kSlots = 16;           // distinct grains per 3-plane window
 constexpr int kTileVolSlots = 512;
 
-template <class R, int KT, int TY>
-struct TileRing {
+template <int TY>
+struct TileGeom {
     static constexpr int kRows = TY + 2;
     static constexpr int kCols = kTileZ + 2;
     static constexpr int kRecs = kRows * kCols;
-    R phi[3][KT][kRecs];
-    int16_t g[3][KT][kRecs];
-    uint8_t cnt[3][kRecs];
+    static constexpr int NT = 32 * TY;
 };
 
-template <class R, int NF, int NT>
-struct TileLists {
-    R val[NF][NT];
-    R lap[NF][NT];
-    int16_t g[NF][NT];
-    uint16_t perm[NT];
-    uint8_t n[NT];      // 0 = bulk / outside, 1..NF = list length, 255 = overflow worklist
-    uint8_t flag[NT];
-    uint8_t m[NT];      // entries of the new record
-};
-
-template <class R, int KT, int NF, int TY>
+template <class R, int KS, int NF, int TY>
 struct TileSmem {
-    TileRing<R, KT, TY> ring;
-    TileLists<R, NF, 32 * TY> lists;
+    using Geo = TileGeom<TY>;
+    R dense[kSlots][3][Geo::kRecs];          // per-slot values of the three ring planes
+    R oval[NF][Geo::NT];                     // new record values (phase B -> C)
     double vol_sum[kTileVolSlots];
+    uint32_t mask[3][Geo::kRecs];            // slot bitmask per record
     int vol_key[kTileVolSlots];
+    int grain_of[kSlots];                    // slot -> grain (-1 = free)
+    int lastpos[kSlots];                     // last window position where the slot's grain occurs
+    int pending[32];                         // grains of the incoming plane that need a slot
     unsigned bucket[NF + 2];
     unsigned base[NF + 2];
     unsigned long long cnt[3];
+    int16_t og[NF][Geo::NT];                 // new record grains (phase B -> C)
+    uint16_t perm[Geo::NT];
+    uint8_t slot[3][KS][Geo::kRecs];         // slot ids in entry order
+    uint8_t cntr[3][Geo::kRecs];             // entries per record
+    uint8_t lslot[NF][Geo::NT];              // the list (slot ids) of every interface voxel
+    uint8_t key[Geo::NT];                    // 0 bulk/outside, 1..NF list length, 255 overflow
+    uint8_t flag[Geo::NT];
+    uint8_t m[Geo::NT];
+    uint8_t bad[3];                          // ring plane holds a grain without slot
+    unsigned npending;
 };
 
 __device__ __forceinline__ void tile_vol_insert(int* keys, double* sums, double* global_acc, int g, double v)
@@ -73,21 +83,44 @@ __device__ __forceinline__ void tile_vol_insert(int* keys, double* sums, double*
     atomicAdd(&global_acc[g], v);
 }
 
-// Stages 2-6 for a list of exactly N entries (compile-time), all arrays in registers.  Writes the
-// new record (m entries, in list order) into the shared-memory list of the voxel; returns m.
-template <class R, int N, int NF, int NT>
-__device__ __forceinline__ int process_list(const StepParams& p, const StepArrays& a, TileLists<R, NF, NT>& L,
-                                            int t, int flag, uint32_t& st)
+// Offsets of the q-th Laplacian stencil element (LaplacianStencil::Set order): 27-point stencils
+// enumerate x, y, z in -1..1; the 7-point stencil keeps the centre and the six faces.
+template <int NS>
+__device__ __forceinline__ constexpr int stencil_dx(int q) { return NS == 27 ? q / 9 - 1 : (q == 0 ? -1 : (q == 6 ? 1 : 0)); }
+template <int NS>
+__device__ __forceinline__ constexpr int stencil_dy(int q) { return NS == 27 ? (q / 3) % 3 - 1 : (q == 1 ? -1 : (q == 5 ? 1 : 0)); }
+template <int NS>
+__device__ __forceinline__ constexpr int stencil_dz(int q) { return NS == 27 ? q % 3 - 1 : (q == 2 ? -1 : (q == 4 ? 1 : 0)); }
+
+// Stages 1b-6 for a list of exactly N fields (compile-time), all arrays in registers: Laplacians
+// from the dense planes, pair kinetics, driving force, projection, merge, finalize.  The new record
+// goes to S.og/S.oval; returns its length.
+template <class R, int N, int NS, int KS, int NF, int TY>
+__device__ __forceinline__ int process_list(const StepParams& p, const StepArrays& a, TileSmem<R, KS, NF, TY>& S,
+                                            int u, int flag, const int (&sl)[3], uint32_t& st)
 {
+    using Geo = TileGeom<TY>;
     constexpr int NP = N * (N - 1) / 2;
-    int g[N];
+    const int rec0 = (u / 32 + 1) * Geo::kCols + (u % 32 + 1);
+    int g[N], s[N];
     R val[N], lap[N];
 #pragma unroll
     for (int k = 0; k < N; k++)
     {
-        g[k] = L.g[k][t];
-        val[k] = L.val[k][t];
-        lap[k] = L.lap[k][t];
+        s[k] = S.lslot[k][u];
+        g[k] = S.grain_of[s[k]];
+        val[k] = S.dense[s[k]][sl[1]][rec0];
+        lap[k] = R(0);
+    }
+    // ---- Laplacians (PhaseField::CalculateDerivativesSR), stencil order ------------------------
+#pragma unroll
+    for (int q = 0; q < NS; q++)
+    {
+        const int pl = sl[stencil_dx<NS>(q) + 1];
+        const int r = rec0 + stencil_dy<NS>(q) * Geo::kCols + stencil_dz<NS>(q);
+        const R w = (R)p.lap_w[q];
+#pragma unroll
+        for (int k = 0; k < N; k++) lap[k] += w * S.dense[s[k]][pl][r];
     }
     // ---- pair kinetics (DoubleObstacle::CalculatePhaseFieldIncrementsSR) ----------------------
     double localN;
@@ -115,7 +148,8 @@ __device__ __forceinline__ int process_list(const StepParams& p, const StepArray
         for (int j = i + 1; j < N; j++)
         {
             const int q = pair_pos(i, j, N);
-            const R scale = (R)sqrt(a.vr[g[i]] * a.vr[g[j]]);
+            const double vra = a.vr[g[i]], vrb = a.vr[g[j]];
+            const R scale = (vra == 1.0 && vrb == 1.0) ? R(1) : (R)sqrt(vra * vrb);   // sqrt(1*1) == 1 exactly
             const R h = R(0.5) * (R(1) + scale) * pref;
             R dphi = sg[q] * ((lap[i] + h * val[i]) - (lap[j] + h * val[j]));
             if (N > 2)
@@ -224,7 +258,7 @@ __device__ __forceinline__ int process_list(const StepParams& p, const StepArray
                         if (w < 0.0) { neg[i] += w; pos[j] += -w; }
                         if (w > 0.0) { pos[i] += w; neg[j] += -w; }
                     }
-                // limits (pos/neg reused as the positive / negative limit of each field)
+                // limits (neg/pos reused as the lower / upper limit of each field)
 #pragma unroll
                 for (int i = 0; i < N; i++)
                 {
@@ -321,8 +355,8 @@ __device__ __forceinline__ int process_list(const StepParams& p, const StepArray
         {
             const R w = (m > 1) ? (R)(vd[i] * norm) : R(1);
             if (!isfinite((double)w)) st |= kStNonFinite;
-            L.g[pos][t] = (int16_t)g[i];
-            L.val[pos][t] = w;
+            S.og[pos][u] = (int16_t)g[i];
+            S.oval[pos][u] = w;
             pos++;
         }
     }
@@ -330,84 +364,103 @@ __device__ __forceinline__ int process_list(const StepParams& p, const StepArray
     return m;
 }
 
-template <class R, int KT, int TY>
-__device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileRing<R, KT, TY>& ring,
-                                           int slot, int xp, int y0, int z0, int t, int nt)
+// Slot of a grain in the window table (-1 if absent).
+__device__ __forceinline__ int find_slot(const int* grain_of, int g)
 {
-    using Ring = TileRing<R, KT, TY>;
+    int r = -1;
+#pragma unroll
+    for (int k = 0; k < kSlots; k++) r = (grain_of[k] == g) ? k : r;
+    return r;
+}
+
+// Bring plane xp (window position wpos) into ring slot `rs`: sparse slot lists, bitmasks and dense
+// per-slot values.  Grains not yet in the window get a slot that no grain of the window uses.
+template <class R, int KS, int NF, int TY>
+__device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileSmem<R, KS, NF, TY>& S,
+                                           int rs, int xp, int wpos, int y0, int z0, int t)
+{
+    using Geo = TileGeom<TY>;
     const long long N = p.n;
     const long long base = (long long)xp * p.ny * p.nz;
     const R* __restrict__ vin = static_cast<const R*>(a.val_in);
-    for (int r = t; r < Ring::kRecs; r += nt)
+    // 1. grains of the incoming plane without a slot
+    for (int r = t; r < Geo::kRecs; r += Geo::NT)
     {
-        const int row = r / Ring::kCols, col = r - (r / Ring::kCols) * Ring::kCols;
+        const int row = r / Geo::kCols, col = r - row * Geo::kCols;
         int yy = y0 - 1 + row; yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy % p.ny : yy);
         int zz = z0 - 1 + col; zz = zz < 0 ? zz + p.nz : (zz >= p.nz ? zz % p.nz : zz);
         const long long v = base + (long long)yy * p.nz + zz;
         const int c = a.cnt_in[v];
-        ring.cnt[slot][r] = (uint8_t)c;
-#pragma unroll
-        for (int s = 0; s < KT; s++)
+        for (int s = 0; s < c; s++)
         {
-            if (s < c)
+            const int g = a.idx_in[s * N + v];
+            if (find_slot(S.grain_of, g) < 0)
             {
-                ring.g[slot][s][r] = a.idx_in[s * N + v];
-                ring.phi[slot][s][r] = vin[s * N + v];
-            }
-        }
-    }
-}
-
-// Append-or-accumulate into a register list of capacity NF (dynamic length n).
-template <class R, int NF>
-__device__ __forceinline__ void list_add(int (&gl)[NF], R (&vl)[NF], R (&ll)[NF], int& n, bool& over, int g, R l,
-                                         bool with_lap)
-{
-    bool found = false;
-#pragma unroll
-    for (int k = 0; k < NF; k++)
-    {
-        if (k < n && gl[k] == g)
-        {
-            if (with_lap) ll[k] += l;
-            found = true;
-        }
-    }
-    if (!found)
-    {
-        if (n < NF)
-        {
-#pragma unroll
-            for (int k = 0; k < NF; k++)
-            {
-                if (k == n)
+                unsigned h = ((unsigned)g * 2654435761u) & 31u;
+                for (int probe = 0; probe < 32; probe++)
                 {
-                    gl[k] = g;
-                    vl[k] = R(0);
-                    ll[k] = with_lap ? l : R(0);
+                    const int k = atomicCAS(&S.pending[h], -1, g);
+                    if (k == -1 || k == g) break;
+                    h = (h + 1) & 31u;
                 }
             }
-            n++;
         }
-        else
+    }
+    __syncthreads();
+    // 2. assign free slots (a slot is free when its grain left the window positions wpos-2.. )
+    if (t == 0)
+    {
+        S.bad[rs] = 0;
+        for (int h = 0; h < 32; h++)
         {
-            over = true;
+            const int g = S.pending[h];
+            if (g < 0) continue;
+            S.pending[h] = -1;
+            int free_slot = -1;
+            for (int k = 0; k < kSlots && free_slot < 0; k++)
+                if (S.grain_of[k] < 0 || S.lastpos[k] < wpos - 2) free_slot = k;
+            if (free_slot < 0) { S.bad[rs] = 1; continue; }
+            S.grain_of[free_slot] = g;
+            S.lastpos[free_slot] = wpos;
         }
+    }
+    __syncthreads();
+    // 3. slot lists, bitmasks, dense values of the incoming plane
+    for (int r = t; r < Geo::kRecs; r += Geo::NT)
+    {
+        const int row = r / Geo::kCols, col = r - row * Geo::kCols;
+        int yy = y0 - 1 + row; yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy % p.ny : yy);
+        int zz = z0 - 1 + col; zz = zz < 0 ? zz + p.nz : (zz >= p.nz ? zz % p.nz : zz);
+        const long long v = base + (long long)yy * p.nz + zz;
+        const int c = a.cnt_in[v];
+#pragma unroll
+        for (int k = 0; k < kSlots; k++) S.dense[k][rs][r] = R(0);
+        uint32_t msk = 0;
+        for (int s = 0; s < c; s++)
+        {
+            const int g = a.idx_in[s * N + v];
+            const int k = find_slot(S.grain_of, g);
+            if (k < 0) { S.bad[rs] = 1; continue; }
+            S.dense[k][rs][r] = vin[s * N + v];
+            S.slot[rs][s][r] = (uint8_t)k;
+            msk |= 1u << k;
+            S.lastpos[k] = wpos;
+        }
+        S.mask[rs][r] = msk;
+        S.cntr[rs][r] = (uint8_t)c;
     }
 }
 
-template <class R, int KS, int KT, int NF, int TY>
+template <class R, int KS, int NF, int TY, int NS>
 __global__ void __launch_bounds__(32 * TY)
 tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int xchunk, int* __restrict__ slow_list,
                  unsigned* __restrict__ slow_count, unsigned slow_cap)
 {
-    constexpr int NT = 32 * TY;
-    using Smem = TileSmem<R, KT, NF, TY>;
-    using Ring = TileRing<R, KT, TY>;
+    using Geo = TileGeom<TY>;
+    using Smem = TileSmem<R, KS, NF, TY>;
+    constexpr int NT = Geo::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
-    auto& ring = S.ring;
-    auto& L = S.lists;
 
     const int tz = threadIdx.x, ty = threadIdx.y, t = ty * 32 + tz;
     const int z0 = blockIdx.x * kTileZ, y0 = blockIdx.y * TY, x0 = blockIdx.z * xchunk;
@@ -417,35 +470,37 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
     const long long plane = (long long)ny * nz;
     const int z = z0 + tz, y = y0 + ty;
     const bool inside = (z < nz) && (y < ny);
-    const R* __restrict__ vin = static_cast<const R*>(a.val_in);
     R* __restrict__ vout = static_cast<R*>(a.val_out);
 
     for (int i = t; i < kTileVolSlots; i += NT) { S.vol_key[i] = -1; S.vol_sum[i] = 0.0; }
+    if (t < kSlots) { S.grain_of[t] = -1; S.lastpos[t] = -1000; }
+    if (t < 32) S.pending[t] = -1;
     if (t < 3) S.cnt[t] = 0ull;
     unsigned wide = 0, ein = 0, eout = 0;
     uint32_t st = 0;
+    __syncthreads();
 
-    load_plane(p, a, ring, 0, x0 == 0 ? nx - 1 : x0 - 1, y0, z0, t, NT);
-    load_plane(p, a, ring, 1, x0, y0, z0, t, NT);
-    const int rec0 = (ty + 1) * Ring::kCols + (tz + 1);
-    const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
-    const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+    load_plane(p, a, S, 0, x0 == 0 ? nx - 1 : x0 - 1, -1, y0, z0, t);
+    __syncthreads();
+    load_plane(p, a, S, 1, x0, 0, y0, z0, t);
+    const int rec0 = (ty + 1) * Geo::kCols + (tz + 1);
 
     for (int x = x0; x < x1; x++)
     {
         const int xi = x - x0;
         const int sl[3] = {xi % 3, (xi + 1) % 3, (xi + 2) % 3};
         if (t <= NF + 1) S.bucket[t] = 0u;
-        load_plane(p, a, ring, sl[2], x == nx - 1 ? 0 : x + 1, y0, z0, t, NT);
         __syncthreads();
+        load_plane(p, a, S, sl[2], x == nx - 1 ? 0 : x + 1, xi + 1, y0, z0, t);
+        __syncthreads();
+        const bool window_bad = S.bad[0] | S.bad[1] | S.bad[2];
 
-        // ---- A: flags, bulk copy, list building -----------------------------------------------
+        // ---- A: flags, bulk copy, candidate discovery --------------------------------------
         const long long v = (long long)x * plane + (long long)y * nz + z;
-        const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
         uint8_t key = 0;
         if (inside)
         {
-            const int c = ring.cnt[sl[1]][rec0];
+            const int c = S.cntr[sl[1]][rec0];
             ein += c;
             int flag = c > 1 ? 2 : 0;
             if (flag == 0)
@@ -453,8 +508,8 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
 #pragma unroll
                 for (int q = 0; q < 27; q++)
                 {
-                    const int r = rec0 + ((q / 3) % 3 - 1) * Ring::kCols + (q % 3 - 1);
-                    if (ring.cnt[sl[q / 9]][r] > 1) flag = 1;
+                    const int r = rec0 + ((q / 3) % 3 - 1) * Geo::kCols + (q % 3 - 1);
+                    if (S.cntr[sl[q / 9]][r] > 1) flag = 1;
                 }
             }
             if (flag == 0)
@@ -462,8 +517,19 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
                 a.cnt_out[v] = (uint8_t)c;
                 for (int s = 0; s < c; s++)
                 {
-                    const int g = s < KT ? ring.g[sl[1]][s < KT ? s : 0][rec0] : a.idx_in[s * N + v];
-                    const R phi = s < KT ? ring.phi[sl[1]][s < KT ? s : 0][rec0] : vin[s * N + v];
+                    int g;
+                    R phi;
+                    if (!window_bad)
+                    {
+                        const int k = S.slot[sl[1]][s][rec0];
+                        g = S.grain_of[k];
+                        phi = S.dense[k][sl[1]][rec0];
+                    }
+                    else
+                    {
+                        g = a.idx_in[s * N + v];
+                        phi = static_cast<const R*>(a.val_in)[s * N + v];
+                    }
                     a.idx_out[s * N + v] = (int16_t)g;
                     vout[s * N + v] = phi;
                     tile_vol_insert(S.vol_key, S.vol_sum, a.vol_acc, g, (double)phi);
@@ -473,76 +539,50 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
             else
             {
                 wide++;
-                int gl[NF];
-                R vl[NF], ll[NF];
-#pragma unroll
-                for (int k = 0; k < NF; k++) { gl[k] = -1; vl[k] = R(0); ll[k] = R(0); }
-                int n = 0;
-                bool over = c > NF;
+                bool over = window_bad || c > NF;
+                int n = c;
                 if (!over)
                 {
+                    uint32_t seen = S.mask[sl[1]][rec0];
+                    uint8_t ls[NF];
 #pragma unroll
-                    for (int k = 0; k < NF; k++)
+                    for (int k = 0; k < NF; k++) ls[k] = k < c ? S.slot[sl[1]][k][rec0] : 0;
+                    // Laplacian pass, then (SIMPLE Laplacian only) the gradient pass of
+                    // CalculateDerivativesSR: new grains in stencil order, neighbour-list order
+                    const int nq = p.ns + p.ng;
+                    for (int q = 0; q < nq && !over; q++)
                     {
-                        if (k < c)
+                        const signed char* d = q < p.ns ? p.lap_d[q] : p.grad_d[q - p.ns];
+                        const int pl = d[0] < 0 ? sl[0] : (d[0] > 0 ? sl[2] : sl[1]);
+                        const int r = rec0 + d[1] * Geo::kCols + d[2];
+                        uint32_t fresh = S.mask[pl][r] & ~seen;
+                        if (fresh)
                         {
-                            gl[k] = k < KT ? ring.g[sl[1]][k < KT ? k : 0][rec0] : a.idx_in[k * N + v];
-                            vl[k] = k < KT ? ring.phi[sl[1]][k < KT ? k : 0][rec0] : vin[k * N + v];
+                            const int cu = S.cntr[pl][r];
+                            for (int s = 0; s < cu; s++)
+                            {
+                                const int k = S.slot[pl][s][r];
+                                if ((fresh >> k) & 1u)
+                                {
+                                    if (n < NF)
+                                    {
+#pragma unroll
+                                        for (int j = 0; j < NF; j++) if (j == n) ls[j] = (uint8_t)k;
+                                        n++;
+                                    }
+                                    else
+                                    {
+                                        over = true;
+                                    }
+                                }
+                            }
+                            seen |= fresh;
                         }
                     }
-                    n = c;
-                }
-                for (int q = 0; q < p.ns && !over; q++)
-                {
-                    const int dx = p.lap_d[q][0], dy = p.lap_d[q][1], dz = p.lap_d[q][2];
-                    const int pl = dx < 0 ? sl[0] : (dx > 0 ? sl[2] : sl[1]);
-                    const int r = rec0 + dy * Ring::kCols + dz;
-                    const R w = (R)p.lap_w[q];
-                    const int cu = ring.cnt[pl][r];
-                    for (int s = 0; s < cu; s++)
+                    if (!over)
                     {
-                        R phi;
-                        int g;
-                        if (s < KT)
-                        {
-                            phi = ring.phi[pl][s][r];
-                            g = ring.g[pl][s][r];
-                        }
-                        else
-                        {
-                            const long long u = (long long)(dx < 0 ? xm : (dx > 0 ? xp : x)) * plane
-                                              + (long long)(dy < 0 ? ym : (dy > 0 ? yp : y)) * nz
-                                              + (dz < 0 ? zm : (dz > 0 ? zp : z));
-                            phi = vin[s * N + u];
-                            g = a.idx_in[s * N + u];
-                        }
-                        if (phi != R(0)) list_add<R, NF>(gl, vl, ll, n, over, g, w * phi, true);
-                    }
-                }
-                for (int q = 0; q < p.ng && !over; q++)
-                {
-                    const int dx = p.grad_d[q][0], dy = p.grad_d[q][1], dz = p.grad_d[q][2];
-                    const int pl = dx < 0 ? sl[0] : (dx > 0 ? sl[2] : sl[1]);
-                    const int r = rec0 + dy * Ring::kCols + dz;
-                    const int cu = ring.cnt[pl][r];
-                    for (int s = 0; s < cu; s++)
-                    {
-                        R phi;
-                        int g;
-                        if (s < KT)
-                        {
-                            phi = ring.phi[pl][s][r];
-                            g = ring.g[pl][s][r];
-                        }
-                        else
-                        {
-                            const long long u = (long long)(dx < 0 ? xm : (dx > 0 ? xp : x)) * plane
-                                              + (long long)(dy < 0 ? ym : (dy > 0 ? yp : y)) * nz
-                                              + (dz < 0 ? zm : (dz > 0 ? zp : z));
-                            phi = vin[s * N + u];
-                            g = a.idx_in[s * N + u];
-                        }
-                        if (phi != R(0)) list_add<R, NF>(gl, vl, ll, n, over, g, R(0), false);
+#pragma unroll
+                        for (int k = 0; k < NF; k++) if (k < n) S.lslot[k][t] = ls[k];
                     }
                 }
                 if (over)
@@ -555,25 +595,15 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
                 else
                 {
                     key = (uint8_t)n;
-#pragma unroll
-                    for (int k = 0; k < NF; k++)
-                    {
-                        if (k < n)
-                        {
-                            L.g[k][t] = (int16_t)gl[k];
-                            L.val[k][t] = vl[k];
-                            L.lap[k][t] = ll[k];
-                        }
-                    }
-                    L.flag[t] = (uint8_t)flag;
+                    S.flag[t] = (uint8_t)flag;
                     atomicAdd(&S.bucket[n], 1u);
                 }
             }
         }
-        L.n[t] = key;
+        S.key[t] = key;
         __syncthreads();
 
-        // ---- bucket lists by length -------------------------------------------------------------
+        // ---- bucket lists by length ---------------------------------------------------------------
         if (t == 0)
         {
             unsigned acc = 0;
@@ -584,41 +614,41 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
         if (key >= 1 && key <= NF)
         {
             const unsigned r = atomicAdd(&S.bucket[key], 1u);
-            L.perm[S.base[key] + r] = (uint16_t)t;
+            S.perm[S.base[key] + r] = (uint16_t)t;
         }
         __syncthreads();
 
-        // ---- B: length-specialised processing ---------------------------------------------------
+        // ---- B: length-specialised processing ------------------------------------------------------
         const unsigned nwork = S.base[NF + 1];
         for (unsigned i = t; i < nwork; i += NT)
         {
-            const int u = L.perm[i];
-            const int n = L.n[u];
-            const int f = L.flag[u];
+            const int u = S.perm[i];
+            const int n = S.key[u];
+            const int f = S.flag[u];
             int m = 0;
             switch (n)
             {
-                case 2: m = process_list<R, 2, NF, NT>(p, a, L, u, f, st); break;
-                case 3: if (NF >= 3) m = process_list<R, (NF >= 3 ? 3 : 2), NF, NT>(p, a, L, u, f, st); break;
-                case 4: if (NF >= 4) m = process_list<R, (NF >= 4 ? 4 : 2), NF, NT>(p, a, L, u, f, st); break;
-                case 5: if (NF >= 5) m = process_list<R, (NF >= 5 ? 5 : 2), NF, NT>(p, a, L, u, f, st); break;
-                case 6: if (NF >= 6) m = process_list<R, (NF >= 6 ? 6 : 2), NF, NT>(p, a, L, u, f, st); break;
-                default: m = process_list<R, 1, NF, NT>(p, a, L, u, f, st); break;
+                case 2: m = process_list<R, 2, NS, KS, NF, TY>(p, a, S, u, f, sl, st); break;
+                case 3: m = process_list<R, (NF >= 3 ? 3 : 2), NS, KS, NF, TY>(p, a, S, u, f, sl, st); break;
+                case 4: m = process_list<R, (NF >= 4 ? 4 : 2), NS, KS, NF, TY>(p, a, S, u, f, sl, st); break;
+                case 5: m = process_list<R, (NF >= 5 ? 5 : 2), NS, KS, NF, TY>(p, a, S, u, f, sl, st); break;
+                case 6: m = process_list<R, (NF >= 6 ? 6 : 2), NS, KS, NF, TY>(p, a, S, u, f, sl, st); break;
+                default: m = process_list<R, 1, NS, KS, NF, TY>(p, a, S, u, f, sl, st); break;
             }
-            L.m[u] = (uint8_t)m;
+            S.m[u] = (uint8_t)m;
         }
         __syncthreads();
 
-        // ---- C: write the new records ---------------------------------------------------------
+        // ---- C: write the new records -----------------------------------------------------------
         if (key >= 1 && key <= NF)
         {
-            const int m = L.m[t] > KS ? KS : L.m[t];
-            if (L.m[t] > KS) st |= kStOverflowK;
+            int m = S.m[t];
+            if (m > KS) { st |= kStOverflowK; m = KS; }
             a.cnt_out[v] = (uint8_t)m;
             for (int s = 0; s < m; s++)
             {
-                const int g = L.g[s][t];
-                const R w = L.val[s][t];
+                const int g = S.og[s][t];
+                const R w = S.oval[s][t];
                 a.idx_out[s * N + v] = (int16_t)g;
                 vout[s * N + v] = w;
                 tile_vol_insert(S.vol_key, S.vol_sum, a.vol_acc, g, (double)w);
@@ -649,9 +679,9 @@ tile_step_kernel(const __grid_constant__ StepParams p, const StepArrays a, int x
         atomicAdd(&a.counters[t == 0 ? kCntWide : (t == 1 ? kCntEntriesIn : kCntEntriesOut)], S.cnt[t]);
 }
 
-// Voxels whose field + candidate list exceeds the tiled kernel's register capacity, through the
-// general per-voxel path (grid-stride over the worklist; the tiled kernel already counted them as
-// wide and counted their input entries).
+// Voxels whose field + candidate list exceeds the tiled kernel's capacity, through the general
+// per-voxel path (grid-stride over the worklist; the tiled kernel already counted them as wide and
+// counted their input entries).
 template <class R, int KS, int KL>
 __global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constant__ StepParams p, const StepArrays a,
                                                             const int* __restrict__ slow_list,
@@ -681,27 +711,22 @@ __global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constan
     if (threadIdx.x == 0 && s_out) atomicAdd(&a.counters[kCntEntriesOut], s_out);
 }
 
-}  // namespace opgpu
-
-namespace opgpu {
-
-constexpr int kTileKT = 4;   // stored slots staged in shared memory
 constexpr int kTileNF = 6;   // register list capacity of the tiled kernel
-constexpr int kTileTY = 8;   // tile rows (blocks of 32 x 8 threads)
+constexpr int kTileTY = 4;   // tile rows (blocks of 32 x 4 threads)
 
-template <class R, int KS, int KL>
-int launch_tiled(const StepParams& p, const StepArrays& a, void* stream)
+template <class R, int KS, int KL, int NS>
+int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream)
 {
-    using Smem = TileSmem<R, kTileKT, kTileNF, kTileTY>;
+    using Smem = TileSmem<R, KS, kTileNF, kTileTY>;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    auto kern = tile_step_kernel<R, KS, kTileKT, kTileNF, kTileTY>;
+    auto kern = tile_step_kernel<R, KS, kTileNF, kTileTY, NS>;
     const size_t smem = sizeof(Smem);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
     const int tz = (p.nz + kTileZ - 1) / kTileZ, ty = (p.ny + kTileTY - 1) / kTileTY;
-    // enough x-chunks for ~8 blocks per SM on small grids, long chunks (halo reuse) on large ones
+    // enough x-chunks for several blocks per SM on small grids, long chunks (halo reuse) on large ones
     int xchunk = (int)((long long)p.nx * tz * ty / (148 * 8));
-    xchunk = xchunk < 2 ? 2 : (xchunk > 16 ? 16 : xchunk);
+    xchunk = xchunk < 2 ? 2 : (xchunk > 32 ? 32 : xchunk);
     const int tx = (p.nx + xchunk - 1) / xchunk;
     e = cudaMemsetAsync(a.slow_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return (int)e;
@@ -710,6 +735,14 @@ int launch_tiled(const StepParams& p, const StepArrays& a, void* stream)
     if (e != cudaSuccess) return (int)e;
     overflow_step_kernel<R, KS, KL><<<148 * 2, 128, 0, s>>>(p, a, a.slow_list, a.slow_count, a.slow_cap);
     return (int)cudaGetLastError();
+}
+
+template <class R, int KS, int KL>
+int launch_tiled(const StepParams& p, const StepArrays& a, void* stream)
+{
+    if (p.ns == 27) return launch_tiled_ns<R, KS, KL, 27>(p, a, stream);
+    if (p.ns == 7) return launch_tiled_ns<R, KS, KL, 7>(p, a, stream);
+    return -1;
 }
 
 template <class R>

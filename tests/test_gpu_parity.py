@@ -102,7 +102,9 @@ def test_k_slot_variants_agree(k_slots):
 @pytest.mark.parametrize("name", ["pairs_dg", "dg_strong", "simple"])
 def test_tiled_kernel_equals_generic_kernel(name, precision):
     """The tiled production kernel (shared-memory halo ring, register lists, overflow worklist for
-    long lists) and the full-grid generic kernel run the same arithmetic: identical states."""
+    long lists) and the full-grid generic kernel run the same per-voxel arithmetic: identical index
+    lists and values equal up to the last-bit effect of the grain-volume summation order (these
+    small grains have VolumeRatio < 1, which feeds the volumes back into the kinetics)."""
     case = CASES[name]
     state = case.initial_state()
     a = Context.from_case(case, precision=precision, k_slots=16, state=state)
@@ -115,7 +117,7 @@ def test_tiled_kernel_equals_generic_kernel(name, precision):
         ca, ia, va = a.download()
         cb, ib, vb = b.download()
         assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
-        assert np.array_equal(va, vb)
+        assert np.max(np.abs(va - vb)) <= (1e-12 if precision == "fp64" else 1e-6)
         ga, gb = a.grains()["volume"], b.grains()["volume"]
         assert np.max(np.abs(ga - gb) / np.maximum(gb, 1.0)) <= 1e-12
     assert a.stats()["wide_total"] == b.stats()["wide_total"]
