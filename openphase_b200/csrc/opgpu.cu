@@ -36,10 +36,21 @@ struct opgpu_ctx {
     int16_t* d_gphase = nullptr;
     int8_t *d_gstage = nullptr, *d_exist = nullptr;
     double *d_dg = nullptr, *d_pair_sigma = nullptr, *d_pair_mu = nullptr;
+    double* d_dg_pair = nullptr;     // limited driving force per grain pair (G <= kMaxPairTableGrains)
+    bool dg_pair_dirty = true;
     uint32_t* d_status = nullptr;
     unsigned long long* d_counters = nullptr;
     int* d_slow_list = nullptr;      // overflow worklist of the tiled kernel (capacity N)
     unsigned* d_slow_count = nullptr;
+    // work buffer of the classify / compute split (see tile_kernel.cuh)
+    void* d_wl_val = nullptr;
+    void* d_wl_lap = nullptr;
+    int16_t* d_wl_g = nullptr;
+    uint8_t* d_wl_flag = nullptr;
+    int* d_bucket = nullptr;
+    unsigned* d_bucket_count = nullptr;
+    long long bucket_cap = 0;
+    int slice = 0;
     int variant = kVariantTiled;
     StepParams sp{};
     bool model_set = false, state_loaded = false, initialized = false;
@@ -246,11 +257,15 @@ void free_grains(opgpu_ctx* c)
 {
     dfree(c->d_vr); dfree(c->d_volume); dfree(c->d_maxvol); dfree(c->d_refvol); dfree(c->d_vol_acc);
     dfree(c->d_gphase); dfree(c->d_gstage); dfree(c->d_exist); dfree(c->d_dg);
-    dfree(c->d_pair_sigma); dfree(c->d_pair_mu);
+    dfree(c->d_pair_sigma); dfree(c->d_pair_mu); dfree(c->d_dg_pair);
     c->d_vr = c->d_volume = c->d_maxvol = c->d_refvol = c->d_vol_acc = nullptr;
     c->d_gphase = nullptr; c->d_gstage = c->d_exist = nullptr;
-    c->d_dg = c->d_pair_sigma = c->d_pair_mu = nullptr;
+    c->d_dg = c->d_pair_sigma = c->d_pair_mu = c->d_dg_pair = nullptr;
+    c->dg_pair_dirty = true;
 }
+
+// Grain counts up to which the limited driving force is tabulated per grain pair (8 * G^2 bytes).
+constexpr int kMaxPairTableGrains = 16384;
 
 // Stencil tables: LaplacianStencil3D_7 / _27a / _LB (include/Containers/LaplacianStencil.h:72-156)
 // and the neighbour sets of GradientStencil1D / 3D / 3D_LB (include/Containers/GradientStencil.h),
@@ -372,6 +387,22 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
     }
     if (dalloc(&ctx->d_slow_list, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
     if (dalloc(&ctx->d_slow_count, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
+    {
+        int xchunk = 0, gz = 0, gy = 0, gx = 0;
+        tiled_geometry(g.nx, g.ny, g.nz, &xchunk, &gz, &gy, &gx);
+        const long long nblocks = (long long)gz * gy * gx;
+        ctx->slice = 32 * kTileRows * xchunk;
+        ctx->bucket_cap = nblocks * ctx->slice;
+        const size_t nl = (size_t)kListCap * ctx->n;
+        if (cudaMalloc(&ctx->d_wl_val, nl * ctx->rsz + 16) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (cudaMalloc(&ctx->d_wl_lap, nl * ctx->rsz + 16) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (dalloc(&ctx->d_wl_g, nl) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (dalloc(&ctx->d_wl_flag, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (dalloc(&ctx->d_bucket, (size_t)(kListCap + 1) * ctx->bucket_cap) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (dalloc(&ctx->d_bucket_count, (size_t)(kListCap + 1) * nblocks) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (cudaMemset(ctx->d_bucket_count, 0, (kListCap + 1) * nblocks * sizeof(unsigned)) != cudaSuccess)
+            return bail(OPGPU_E_CUDA);
+    }
     if (dalloc(&ctx->d_status, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
     if (dalloc(&ctx->d_counters, kNumCounters) != cudaSuccess) return bail(OPGPU_E_CUDA);
     cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
@@ -402,6 +433,8 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     dfree(ctx->d_slow_list);
     dfree(ctx->d_slow_count);
+    dfree(ctx->d_wl_val); dfree(ctx->d_wl_lap); dfree(ctx->d_wl_g); dfree(ctx->d_wl_flag);
+    dfree(ctx->d_bucket); dfree(ctx->d_bucket_count);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -437,6 +470,7 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
     }
     ctx->nvf = m->nucleus_volume_factor > 0.0 ? m->nucleus_volume_factor : 1.0;
     ctx->model_set = true;
+    ctx->dg_pair_dirty = true;
     return OPGPU_OK;
 }
 
@@ -528,6 +562,7 @@ extern "C" uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG)
     CK(cudaMemcpyAsync(ctx->d_dg, dG, ctx->G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->sp.use_dg = 1;
+    ctx->dg_pair_dirty = true;
     return OPGPU_OK;
 }
 
@@ -623,6 +658,14 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
     if (ctx->sp.use_dg && !ctx->d_dg) return fail(ctx, OPGPU_E_STATE, "opgpu_step: driving force enabled without values");
     StepParams sp = ctx->sp;
     sp.dt = dt;
+    const bool pair_table = sp.use_dg && ctx->G <= kMaxPairTableGrains;
+    if (pair_table && ctx->dg_pair_dirty)
+    {
+        if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, (size_t)ctx->G * ctx->G));
+        const int rc = launch_dg_pair(sp, ctx->d_dg, ctx->d_gphase, ctx->d_dg_pair, ctx->stream);
+        if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("driving-force table: ") + cudaGetErrorString((cudaError_t)rc));
+        ctx->dg_pair_dirty = false;
+    }
     for (int s = 0; s < nsteps; s++)
     {
         const int in = ctx->cur, out = 1 - ctx->cur;
@@ -631,8 +674,12 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
         a.cnt_out = ctx->cnt[out]; a.idx_out = ctx->idx[out]; a.val_out = ctx->val[out];
         a.vr = ctx->d_vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
         a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
+        a.dg_pair = pair_table ? ctx->d_dg_pair : nullptr;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
+        a.wl_val = ctx->d_wl_val; a.wl_lap = ctx->d_wl_lap; a.wl_g = ctx->d_wl_g; a.wl_flag = ctx->d_wl_flag;
+        a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
+        a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;
         if (ctx->timing)
         {
             if (ctx->ev_pool.size() < 2 * (ctx->ev_used + 1))

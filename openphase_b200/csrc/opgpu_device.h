@@ -74,6 +74,7 @@ struct StepArrays {
     const double* dg;          // [G] or null
     const double* pair_sigma;  // [G*G] or null
     const double* pair_mu;     // [G*G] or null
+    const double* dg_pair;     // [G*G] limited driving force per grain pair, or null (evaluated in place)
     double* vol_acc;           // [G] volume accumulator of the output state (zeroed by the caller)
     uint32_t* status;          // soft status bits
     unsigned long long* counters;  // kNumCounters
@@ -81,7 +82,33 @@ struct StepArrays {
     int* slow_list;            // [slow_cap]
     unsigned* slow_count;      // reset by the launcher before every step
     unsigned slow_cap;
+    // work buffer between the classify kernel and the per-length compute kernels
+    void* wl_val;              // [kListCap][N] values of the list fields (own fields, then candidates)
+    void* wl_lap;              // [kListCap][N] their Laplacians
+    int16_t* wl_g;             // [kListCap][N] their grains
+    uint8_t* wl_flag;          // [N] interface flag of the voxel (1 or 2)
+    int* bucket;               // [kListCap + 1][bucket_cap] voxels per list length, block-private slices
+    unsigned* bucket_count;    // [kListCap + 1][max blocks] entries per slice
+    long long bucket_cap;
+    int slice;                 // entries per classify-block slice
 };
+
+constexpr int kListCap = 6;    // list capacity of the split kernels (longer lists: overflow worklist)
+constexpr int kTileRows = 4;   // tile rows of the classify kernel (tiles of 32 x kTileRows voxels)
+
+// Launch geometry of the classify kernel: tiles of 32 (z) x kTileRows (y) voxels marching over
+// `xchunk` x-planes; enough x-chunks for several blocks per SM on small grids, long chunks (halo
+// reuse) on large ones.  slice = voxels one block can append to a bucket.
+inline void tiled_geometry(int nx, int ny, int nz, int* xchunk, int* gz, int* gy, int* gx)
+{
+    const int tzb = (nz + 31) / 32, tyb = (ny + kTileRows - 1) / kTileRows;
+    long long xc = (long long)nx * tzb * tyb / (148 * 8);
+    xc = xc < 2 ? 2 : (xc > 32 ? 32 : xc);
+    *xchunk = (int)xc;
+    *gz = tzb;
+    *gy = tyb;
+    *gx = (int)((nx + xc - 1) / xc);
+}
 
 enum { kVariantTiled = 0, kVariantGeneric = 1 };
 
@@ -89,5 +116,8 @@ enum { kVariantTiled = 0, kVariantGeneric = 1 };
 // tiled production kernel or the full-grid generic kernel (same results, used for validation).
 int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream);
 int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream);
+// Fill out[a*G+b] with the limited driving force of every grain pair (defined in step_f64.cu, so
+// that it is compiled exactly like the in-place evaluation of the FP64 form).
+int launch_dg_pair(const StepParams& p, const double* dg, const int16_t* gphase, double* out, void* stream);
 
 }  // namespace opgpu

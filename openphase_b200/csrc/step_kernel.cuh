@@ -1,7 +1,6 @@
-// The fused multiphase-field time step for sm_100a: one thread per voxel, one launch per step.
+// Per-voxel arithmetic of the fused multiphase-field time step, and the full-grid generic kernel.
 //
-// For every voxel the kernel performs, in registers/local memory, what the reference spreads over
-// five grid passes:
+// For one voxel, what the reference spreads over five grid passes:
 //   1. derivatives + candidates   PhaseField::CalculateDerivativesSR  (src/PhaseField.cpp:566-615)
 //   2. pairwise kinetics          DoubleObstacle::CalculatePhaseFieldIncrementsSR
 //                                 (src/DoubleObstacle.cpp:502-571)
@@ -9,14 +8,15 @@
 //   4. simplex projection         PhaseField::NormalizeIncrementsSR (src/PhaseField.cpp:1351-1561)
 //   5. merge + finalize           PhaseField::MergeIncrementsSR (:1268-1299), NodePF::finalize
 //                                 (include/Containers/NodePF.h:214-255)
-// and it accumulates the grain volumes of the new state (PhaseField::CalculateGrainsVolume,
-// src/PhaseField.cpp:812-951) through a per-block shared-memory table.  The flags of
-// PhaseField::SetFlagsSR are derived from neighbour counts on the fly, the periodic boundary
-// copies (BoundaryConditions::SetX/Y/Z) become index wrap-around.
+// Stage 1 differs between the kernels (global-memory scan here, shared-memory dense planes in the
+// tiled kernel); stages 2-5 are `list_step`, shared by both.  The flags of PhaseField::SetFlagsSR
+// are derived from neighbour counts, the periodic boundary copies become index wrap-around, and
+// the grain volumes of the new state (PhaseField::CalculateGrainsVolume, src/PhaseField.cpp:812-951)
+// accumulate through per-block shared-memory tables.
 //
-// Exactness: in the FP64 form (this header compiled with --fmad=false) every floating-point
-// expression is evaluated in the reference's order, so results are bit-identical to the
-// reference except for tanh (CUDA vs. libm, a few ulp) and the grain-volume summation order.
+// Exactness: in the FP64 form (compiled with --fmad=false) every floating-point expression is
+// evaluated in the reference's order, so results are bit-identical to the reference except for
+// tanh (CUDA vs. libm, a few ulp) and the grain-volume summation order.
 #pragma once
 #include <cfloat>
 #include <cstdint>
@@ -51,13 +51,28 @@ __device__ __forceinline__ double pair_mobility(const StepParams& p, const StepA
     return p.mu_p[a.gphase[ga] * p.nphases + a.gphase[gb]];
 }
 
+// The driving force of a grain pair after the tanh limiter (src/DrivingForce.cpp:548-583):
+// allowed*tanh((dG_b - dG_a)/allowed).  It depends on the pair only, so the step reads it from a
+// G*G table filled once per parameter change (same arithmetic), else evaluates it in place.
+__device__ __forceinline__ double limited_force(const StepParams& p, const StepArrays& a, int ga, int gb)
+{
+    if (a.dg_pair) return a.dg_pair[(long long)ga * p.ngrains + gb];
+    double locdG = a.dg[gb] - a.dg[ga];
+    if (p.limiting)
+    {
+        const double allowed = p.allowed_p[a.gphase[ga] * p.nphases + a.gphase[gb]];
+        locdG = allowed * tanh(locdG / allowed);
+    }
+    return locdG;
+}
+
 // Per-block grain-volume table in shared memory.
 constexpr int kVolSlots = 1024;
 
-__device__ __forceinline__ void vol_insert(int* keys, double* sums, double* global_acc, int g, double v)
+__device__ __forceinline__ void vol_insert_n(int* keys, double* sums, int nslots, double* global_acc, int g, double v)
 {
-    unsigned h = ((unsigned)g * 2654435761u) & (kVolSlots - 1);
-    for (int probe = 0; probe < kVolSlots; probe++)
+    unsigned h = ((unsigned)g * 2654435761u) & (unsigned)(nslots - 1);
+    for (int probe = 0; probe < nslots; probe++)
     {
         const int k = atomicCAS(&keys[h], -1, g);
         if (k == -1 || k == g)
@@ -65,363 +80,421 @@ __device__ __forceinline__ void vol_insert(int* keys, double* sums, double* glob
             atomicAdd(&sums[h], v);
             return;
         }
-        h = (h + 1) & (kVolSlots - 1);
+        h = (h + 1) & (unsigned)(nslots - 1);
     }
     atomicAdd(&global_acc[g], v);
 }
 
-// One voxel of the step, reading its 3x3x3 neighbourhood straight from global memory, with the
-// field+candidate list and the pair increments in local memory (capacity KL entries).  This is
-// the general path: the full-grid reference kernel below and the overflow kernel of the tiled step
-// (voxels whose lists exceed the tiled kernel's register capacity) both run it.
-template <class R, int KS, int KL>
-__device__ __forceinline__ void voxel_step_generic(const StepParams& p, const StepArrays& a, long long v,
-                                                   int* s_key, double* s_sum, unsigned& wide, unsigned& ein,
-                                                   unsigned& eout, uint32_t& st, bool count_in)
+// Working arrays of one voxel: element k of an array at base[k*stride] (stride 1 for per-thread
+// local arrays, the block size for a column of shared memory).
+template <class R>
+struct ListScratch {
+    int16_t* g;      // [KL] grain indices (in: list, out: new record)
+    R* val;          // [KL] values        (in: list, out: new record)
+    R* lap;          // [KL] Laplacians
+    R* sg;           // [KL*(KL-1)/2] pair energies
+    double* pv;      // [KL*(KL-1)/2] pair increments
+    double* pos;     // [KL] positive increments / upper limits
+    double* neg;     // [KL] negative increments / lower limits
+    int stride;
+};
+
+// Stages 2-5 for a list of n fields (own fields first, then candidates, as CalculateDerivativesSR
+// leaves them) with their Laplacians.  Leaves the new record (the fields that survive finalize, in
+// list order) in sc.g / sc.val and returns its length.
+template <class R>
+__device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& a, const ListScratch<R>& sc, int n,
+                                         int flag, uint32_t& st)
 {
-    const long long N = p.n;
+    const int S = sc.stride;
+#define G_(k) sc.g[(k) * S]
+#define V_(k) sc.val[(k) * S]
+#define L_(k) sc.lap[(k) * S]
+#define SG_(q) sc.sg[(q) * S]
+#define PV_(q) sc.pv[(q) * S]
+#define POS_(k) sc.pos[(k) * S]
+#define NEG_(k) sc.neg[(k) * S]
+    // ---- 2. pair kinetics -----------------------------------------------------------------------
+    double localN;
+    if (p.consider_nucleus_volume)
     {
-        const uint8_t* __restrict__ cnt = a.cnt_in;
-        const int16_t* __restrict__ gin = a.idx_in;
-        const R* __restrict__ vin = static_cast<const R*>(a.val_in);
-        R* __restrict__ vout = static_cast<R*>(a.val_out);
-
-        const int nx = p.nx, ny = p.ny, nz = p.nz;
-        const int z = (int)(v % nz);
-        const long long t = v / nz;
-        const int y = (int)(t % ny);
-        const int x = (int)(t / ny);
-        const long long plane = (long long)ny * nz;
-        long long X[3], Y[3], Z[3];
-        X[0] = (long long)(x == 0 ? nx - 1 : x - 1) * plane; X[1] = (long long)x * plane;
-        X[2] = (long long)(x == nx - 1 ? 0 : x + 1) * plane;
-        Y[0] = (long long)(y == 0 ? ny - 1 : y - 1) * nz; Y[1] = (long long)y * nz;
-        Y[2] = (long long)(y == ny - 1 ? 0 : y + 1) * nz;
-        Z[0] = (z == 0 ? nz - 1 : z - 1); Z[1] = z; Z[2] = (z == nz - 1 ? 0 : z + 1);
-
-        const int c = cnt[v];
-        ein = c;
-        int flag = c > 1 ? 2 : 0;
-        if (flag == 0)
+        localN = 0.0;
+        for (int k = 0; k < n; k++) localN += a.vr[G_(k)];
+    }
+    else
+    {
+        localN = (double)n;
+    }
+    const R norm_1 = (R)(1.0 / localN);
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) SG_(pair_pos(i, j, n)) = (R)pair_energy(p, a, G_(i), G_(j));
+    const R pref = (R)p.pref_do;
+    for (int i = 0; i < n; i++)
+    {
+        const int gi = G_(i);
+        const double vri = a.vr[gi];
+        const R vali = V_(i), lapi = L_(i);
+        for (int j = i + 1; j < n; j++)
         {
-            for (int q = 0; q < 27 && flag == 0; q++)
+            const int gj = G_(j);
+            const int q = pair_pos(i, j, n);
+            const double vrj = a.vr[gj];
+            const R scale = (vri == 1.0 && vrj == 1.0) ? R(1) : (R)sqrt(vri * vrj);   // sqrt(1*1) == 1
+            const R h = R(0.5) * (R(1) + scale) * pref;
+            const R valj = V_(j);
+            R dphi = SG_(q) * ((lapi + h * vali) - (L_(j) + h * valj));
+            if (n > 2)
             {
-                const long long u = X[q / 9] + Y[(q / 3) % 3] + Z[q % 3];
-                if (cnt[u] > 1) flag = 1;
+                for (int k = 0; k < n; k++)
+                {
+                    if (k == i || k == j) continue;
+                    const R sbk = SG_(j < k ? pair_pos(j, k, n) : pair_pos(k, j, n));
+                    const R sak = SG_(i < k ? pair_pos(i, k, n) : pair_pos(k, i, n));
+                    const R valk = V_(k);
+                    dphi += (sbk - sak) * (L_(k) + h * valk);
+                    if (p.tj_factor != 0.0 || scale < R(1))
+                    {
+                        const int pA = a.gphase[gi], pB = a.gphase[gj], pG = a.gphase[G_(k)];
+                        const int P = p.nphases;
+                        const R tj = (R)dmax_ref(p.tj_factor, (double)(R(1) - scale));
+                        dphi += tj * pref
+                              * (((R)p.sigma_p[pA * P + pB] + (R)p.sigma_p[pB * P + pG]) + (R)p.sigma_p[pA * P + pG])
+                              * (vali * valk - valj * valk);
+                    }
+                }
+            }
+            dphi *= (R)pair_mobility(p, a, gi, gj) * norm_1 * scale;
+            PV_(q) = (double)dphi;
+        }
+    }
+    // ---- 3. driving force (interface voxels only) ----------------------------------------------
+    if (p.use_dg && flag == 2)
+    {
+        for (int i = 0; i < n; i++)
+        {
+            const int gi = G_(i);
+            const double vi = (double)V_(i);
+            for (int j = i + 1; j < n; j++)
+            {
+                const int gj = G_(j);
+                const double locdG = limited_force(p, a, gi, gj);
+                double norm = sqrt(vi * (double)V_(j));
+                if (a.gstage[gi] == 1 || a.gstage[gj] == 1) norm += 1.0e-6;
+                const double dpsi = locdG * (double)(R)pair_mobility(p, a, gi, gj) * norm * p.pref_df;
+                PV_(pair_pos(i, j, n)) += dpsi;
             }
         }
-
-        if (flag == 0)
+    }
+    // ---- 4. projection (NormalizeIncrementsSR) ---------------------------------------------------
+    const double dt = p.dt;
+    const int np = n * (n - 1) / 2;
+    if (np == 1)
+    {
+        const double valueA = (PV_(0) + 0.0) * dt;
+        const double old_value = (double)V_(0);
+        if ((old_value == 0.0 && valueA < 0.0) || (old_value == 1.0 && valueA > 0.0))
         {
-            // bulk voxel: the state is carried over unchanged (it is not touched by any stage)
-            a.cnt_out[v] = (uint8_t)c;
-            for (int s = 0; s < c; s++)
-            {
-                const int g = gin[s * N + v];
-                const R phi = vin[s * N + v];
-                a.idx_out[s * N + v] = (int16_t)g;
-                vout[s * N + v] = phi;
-                vol_insert(s_key, s_sum, a.vol_acc, g, (double)phi);
-            }
-            eout = c;
+            PV_(0) = 0.0;
         }
         else
         {
-            wide = 1;
-            // ---- 1. own entries, then candidates, with Laplacians (stencil order) -----------
-            int n = 0;
-            int gL[KL];
-            R val[KL];
-            R lap[KL];
-            for (int s = 0; s < c; s++)
-            {
-                gL[n] = gin[s * N + v];
-                val[n] = vin[s * N + v];
-                lap[n] = R(0);
-                n++;
-            }
-            for (int q = 0; q < p.ns; q++)
-            {
-                const long long u = X[p.lap_d[q][0] + 1] + Y[p.lap_d[q][1] + 1] + Z[p.lap_d[q][2] + 1];
-                const R w = (R)p.lap_w[q];
-                const int cu = cnt[u];
-                for (int s = 0; s < cu; s++)
-                {
-                    const R phi = vin[s * N + u];
-                    if (phi != R(0))
-                    {
-                        const int g = gin[s * N + u];
-                        const R l = w * phi;
-                        int f = 0;
-                        while (f < n && gL[f] != g) f++;
-                        if (f < n) lap[f] += l;
-                        else if (n < KL) { gL[n] = g; val[n] = R(0); lap[n] = l; n++; }
-                        else st |= kStOverflowList;
-                    }
-                }
-            }
-            // the gradient pass of CalculateDerivativesSR appends indices it meets first
-            for (int q = 0; q < p.ng; q++)
-            {
-                const long long u = X[p.grad_d[q][0] + 1] + Y[p.grad_d[q][1] + 1] + Z[p.grad_d[q][2] + 1];
-                const int cu = cnt[u];
-                for (int s = 0; s < cu; s++)
-                {
-                    const R phi = vin[s * N + u];
-                    if (phi != R(0))
-                    {
-                        const int g = gin[s * N + u];
-                        int f = 0;
-                        while (f < n && gL[f] != g) f++;
-                        if (f == n)
-                        {
-                            if (n < KL) { gL[n] = g; val[n] = R(0); lap[n] = R(0); n++; }
-                            else st |= kStOverflowList;
-                        }
-                    }
-                }
-            }
-
-            // ---- 2. double-obstacle pair kinetics -------------------------------------------
-            constexpr int KP = KL * (KL - 1) / 2;
-            // pair increments are kept in FP64 from here on (the FP32 form widens the kinetics'
-            // result so that the projection's sums and limiter run as in the FP64 form)
-            double pv[KP];
-            R sg[KP];
-            R mg[KP];
-            double localN;
-            if (p.consider_nucleus_volume)
-            {
-                localN = 0.0;
-                for (int q = 0; q < n; q++) localN += a.vr[gL[q]];
-            }
-            else
-            {
-                localN = (double)n;
-            }
-            const R norm_1 = (R)(1.0 / localN);
-            for (int i = 0; i < n; i++)
-            for (int j = i + 1; j < n; j++)
-            {
-                const int q = pair_pos(i, j, n);
-                sg[q] = (R)pair_energy(p, a, gL[i], gL[j]);
-                mg[q] = (R)pair_mobility(p, a, gL[i], gL[j]);
-            }
-            const R pref = (R)p.pref_do;
-            for (int i = 0; i < n; i++)
-            for (int j = i + 1; j < n; j++)
-            {
-                const int q = pair_pos(i, j, n);
-                const R scale = (R)sqrt(a.vr[gL[i]] * a.vr[gL[j]]);
-                const R h = R(0.5) * (R(1) + scale) * pref;
-                R dphi = sg[q] * ((lap[i] + h * val[i]) - (lap[j] + h * val[j]));
-                if (n > 2)
-                {
-                    for (int k = 0; k < n; k++)
-                    {
-                        if (k == i || k == j) continue;
-                        const R sbk = sg[j < k ? pair_pos(j, k, n) : pair_pos(k, j, n)];
-                        const R sak = sg[i < k ? pair_pos(i, k, n) : pair_pos(k, i, n)];
-                        dphi += (sbk - sak) * (lap[k] + h * val[k]);
-                        if (p.tj_factor != 0.0 || scale < R(1))
-                        {
-                            const int pA = a.gphase[gL[i]], pB = a.gphase[gL[j]], pG = a.gphase[gL[k]];
-                            const int P = p.nphases;
-                            const R tj = (R)dmax_ref(p.tj_factor, (double)(R(1) - scale));
-                            dphi += tj * pref
-                                  * (((R)p.sigma_p[pA * P + pB] + (R)p.sigma_p[pB * P + pG]) + (R)p.sigma_p[pA * P + pG])
-                                  * (val[i] * val[k] - val[j] * val[k]);
-                        }
-                    }
-                }
-                dphi *= mg[q] * norm_1 * scale;
-                pv[q] = (double)dphi;
-            }
-
-            // ---- 3. driving force (interface voxels only) -----------------------------------
-            if (p.use_dg && flag == 2)
-            {
-                const int P = p.nphases;
-                for (int i = 0; i < n; i++)
-                for (int j = i + 1; j < n; j++)
-                {
-                    const int q = pair_pos(i, j, n);
-                    const int gi = gL[i], gj = gL[j];
-                    double locdG = a.dg[gj] - a.dg[gi];
-                    double norm = sqrt((double)val[i] * (double)val[j]);
-                    if (a.gstage[gi] == 1 || a.gstage[gj] == 1) norm += 1.0e-6;
-                    if (p.limiting)
-                    {
-                        const double allowed = p.allowed_p[a.gphase[gi] * P + a.gphase[gj]];
-                        locdG = allowed * tanh(locdG / allowed);
-                    }
-                    const double dpsi = locdG * (double)mg[q] * norm * p.pref_df;
-                    pv[q] += dpsi;
-                }
-            }
-
-            // ---- 4. projection of the increments (NormalizeIncrementsSR) --------------------
-            const double dt = p.dt;
-            const int np = n * (n - 1) / 2;
-            if (np == 1)
-            {
-                const double valueA = ((double)pv[0] + 0.0) * dt;
-                const double old_value = (double)val[0];
-                if ((old_value == 0.0 && valueA < 0.0) || (old_value == 1.0 && valueA > 0.0))
-                {
-                    pv[0] = 0.0;
-                }
-                else
-                {
-                    const double new_value = old_value + valueA;
-                    double norm = 1.0;
-                    if (new_value < 0.0) norm *= -old_value / valueA;
-                    else if (new_value > 1.0) norm *= (1.0 - old_value) / valueA;
-                    if (norm > DBL_EPSILON) pv[0] *= norm;
-                    else pv[0] = 0.0;
-                }
-            }
-            else if (np > 1)
-            {
-                for (int i = 0; i < n; i++)
-                {
-                    double dpsi = 0.0;
-                    for (int j = 0; j < n; j++)
-                    {
-                        if (j == i) continue;
-                        dpsi += (i < j) ? (double)pv[pair_pos(i, j, n)] : (double)pv[pair_pos(j, i, n)] * (-1.0);
-                    }
-                    if (((double)val[i] == 0.0 && dpsi < 0.0) || ((double)val[i] == 1.0 && dpsi > 0.0))
-                    {
-                        for (int j = 0; j < n; j++)
-                        {
-                            if (j == i) continue;
-                            pv[i < j ? pair_pos(i, j, n) : pair_pos(j, i, n)] = 0.0;
-                        }
-                    }
-                }
-                bool any = false;
-                for (int q = 0; q < np; q++) any |= (pv[q] != 0.0);
-                if (any)
-                {
-                    double pos[KL], neg[KL], limP[KL], limN[KL];
-                    int iterations = 0;
-                    bool needed = true;
-                    while (needed)
-                    {
-                        iterations++;
-                        needed = false;
-                        for (int i = 0; i < n; i++) { pos[i] = 0.0; neg[i] = 0.0; }
-                        for (int i = 0; i < n; i++)
-                        for (int j = i + 1; j < n; j++)
-                        {
-                            const double w = (double)pv[pair_pos(i, j, n)];
-                            if (w < 0.0) { neg[i] += w; pos[j] += -w; }
-                            if (w > 0.0) { pos[i] += w; neg[j] += -w; }
-                        }
-                        for (int i = 0; i < n; i++)
-                        {
-                            const double vi = (double)val[i];
-                            const double newPF = vi + (pos[i] + neg[i]) * dt;
-                            limN[i] = 1.0;
-                            limP[i] = 1.0;
-                            if (newPF < 0.0) limN[i] = dmin_ref(1.0, -(vi + pos[i] * dt) / (neg[i] * dt));
-                            if (newPF > 1.0) limP[i] = dmin_ref(1.0, (1.0 - (vi + neg[i] * dt)) / (pos[i] * dt));
-                        }
-                        for (int i = 0; i < n; i++)
-                        for (int j = i + 1; j < n; j++)
-                        {
-                            const int q = pair_pos(i, j, n);
-                            if (pv[q] < 0.0)
-                            {
-                                const double lim = dmin_ref(limN[i], limP[j]);
-                                pv[q] *= lim;
-                                if (lim < 1.0) needed = true;
-                            }
-                            if (pv[q] > 0.0)
-                            {
-                                const double lim = dmin_ref(limP[i], limN[j]);
-                                pv[q] *= lim;
-                                if (lim < 1.0) needed = true;
-                            }
-                        }
-                        if (iterations > 24)
-                        {
-                            if (needed) st |= kStLimiterCap;
-                            needed = false;
-                        }
-                    }
-                    for (int q = 0; q < np; q++)
-                        if (fabs(pv[q] * dt) < DBL_EPSILON) pv[q] = 0.0;
-                    // plausibility check (a warning in the reference)
-                    for (int i = 0; i < n; i++) pos[i] = (double)val[i];
-                    for (int i = 0; i < n; i++)
-                    for (int j = i + 1; j < n; j++)
-                    {
-                        const double w = (double)pv[pair_pos(i, j, n)];
-                        if (w != 0.0) { pos[i] += w * dt; pos[j] += -w * dt; }
-                    }
-                    for (int i = 0; i < n; i++)
-                        if (pos[i] < -(double)FLT_EPSILON || pos[i] > 1.0 + (double)FLT_EPSILON) st |= kStNormalizeWarn;
-                }
-            }
-
-            // ---- 5. merge (volume conserving, pair by pair) ---------------------------------
-            // accumulated in FP64; the FP32 form rounds only when the record is stored
-            double vd[KL];
-            for (int i = 0; i < n; i++) vd[i] = (double)val[i];
-            for (int i = 0; i < n; i++)
-            for (int j = i + 1; j < n; j++)
-            {
-                const double w = pv[pair_pos(i, j, n)];
-                const double value = 1.0 * (w + 0.0) * dt;
-                if (fabs(value) >= DBL_EPSILON)
-                {
-                    vd[i] += value;
-                    vd[j] += -value;
-                }
-            }
-
-            // ---- 6. finalize: snap, erase, renormalise --------------------------------------
-            double total = 0.0;
-            int m = 0;
-            const double hi_snap = 1.0 - p.eps_snap;
-            const double lo_snap = 0.0 + p.eps_snap;
-            for (int i = 0; i < n; i++)
-            {
-                double w = vd[i];
-                bool erase = false;
-                if (w >= hi_snap) w = 1.0;
-                if (w <= lo_snap) { w = 0.0; erase = true; }
-                total += w;
-                if (!erase) { gL[m] = gL[i]; vd[m] = w; m++; }
-            }
-            if (m > 1)
-            {
-                const double norm = 1.0 / total;
-                for (int i = 0; i < m; i++) val[i] = (R)(vd[i] * norm);
-            }
-            else if (m == 1)
-            {
-                val[0] = R(1);
-            }
-            else
-            {
-                st |= kStEmptyVoxel;
-            }
-            if (m > KS) { st |= kStOverflowK; m = KS; }
-            a.cnt_out[v] = (uint8_t)m;
-            for (int i = 0; i < m; i++)
-            {
-                if (!isfinite((double)val[i])) st |= kStNonFinite;
-                a.idx_out[i * N + v] = (int16_t)gL[i];
-                vout[i * N + v] = val[i];
-                vol_insert(s_key, s_sum, a.vol_acc, gL[i], (double)val[i]);
-            }
-            eout = m;
+            const double new_value = old_value + valueA;
+            double norm = 1.0;
+            if (new_value < 0.0) norm *= -old_value / valueA;
+            else if (new_value > 1.0) norm *= (1.0 - old_value) / valueA;
+            if (norm > DBL_EPSILON) PV_(0) *= norm;
+            else PV_(0) = 0.0;
         }
     }
-    if (!count_in) { ein = 0; }
+    else if (np > 1)
+    {
+        for (int i = 0; i < n; i++)
+        {
+            double dpsi = 0.0;
+            for (int j = 0; j < n; j++)
+            {
+                if (j == i) continue;
+                dpsi += (i < j) ? PV_(pair_pos(i, j, n)) : PV_(pair_pos(j, i, n)) * (-1.0);
+            }
+            const double vi = (double)V_(i);
+            if ((vi == 0.0 && dpsi < 0.0) || (vi == 1.0 && dpsi > 0.0))
+            {
+                for (int j = 0; j < n; j++)
+                {
+                    if (j == i) continue;
+                    PV_(i < j ? pair_pos(i, j, n) : pair_pos(j, i, n)) = 0.0;
+                }
+            }
+        }
+        bool any = false;
+        for (int q = 0; q < np; q++) any |= (PV_(q) != 0.0);
+        if (any)
+        {
+            for (int it = 1; it <= 25; it++)
+            {
+                for (int i = 0; i < n; i++) { POS_(i) = 0.0; NEG_(i) = 0.0; }
+                for (int i = 0; i < n; i++)
+                    for (int j = i + 1; j < n; j++)
+                    {
+                        const double w = PV_(pair_pos(i, j, n));
+                        if (w < 0.0) { NEG_(i) += w; POS_(j) += -w; }
+                        if (w > 0.0) { POS_(i) += w; NEG_(j) += -w; }
+                    }
+                // limits: NEG_ becomes the lower limit, POS_ the upper limit of each field
+                for (int i = 0; i < n; i++)
+                {
+                    const double vi = (double)V_(i);
+                    const double pi = POS_(i), ni = NEG_(i);
+                    const double newPF = vi + (pi + ni) * dt;
+                    double limN = 1.0, limP = 1.0;
+                    if (newPF < 0.0) limN = dmin_ref(1.0, -(vi + pi * dt) / (ni * dt));
+                    if (newPF > 1.0) limP = dmin_ref(1.0, (1.0 - (vi + ni * dt)) / (pi * dt));
+                    NEG_(i) = limN;
+                    POS_(i) = limP;
+                }
+                bool needed = false;
+                for (int i = 0; i < n; i++)
+                    for (int j = i + 1; j < n; j++)
+                    {
+                        const int q = pair_pos(i, j, n);
+                        double w = PV_(q);
+                        if (w < 0.0)
+                        {
+                            const double lim = dmin_ref(NEG_(i), POS_(j));
+                            w *= lim;
+                            if (lim < 1.0) needed = true;
+                        }
+                        if (w > 0.0)
+                        {
+                            const double lim = dmin_ref(POS_(i), NEG_(j));
+                            w *= lim;
+                            if (lim < 1.0) needed = true;
+                        }
+                        PV_(q) = w;
+                    }
+                if (!needed) break;
+                if (it == 25) st |= kStLimiterCap;
+            }
+            for (int q = 0; q < np; q++)
+                if (fabs(PV_(q) * dt) < DBL_EPSILON) PV_(q) = 0.0;
+            // plausibility check (a warning in the reference); POS_ holds the trial values
+            for (int i = 0; i < n; i++) POS_(i) = (double)V_(i);
+            for (int i = 0; i < n; i++)
+                for (int j = i + 1; j < n; j++)
+                {
+                    const double w = PV_(pair_pos(i, j, n));
+                    if (w != 0.0) { POS_(i) += w * dt; POS_(j) += -w * dt; }
+                }
+            for (int i = 0; i < n; i++)
+            {
+                const double c = POS_(i);
+                if (c < -(double)FLT_EPSILON || c > 1.0 + (double)FLT_EPSILON) st |= kStNormalizeWarn;
+            }
+        }
+    }
+    // ---- 5. merge (accumulated in FP64, NEG_ holds the new values) and finalize -----------------
+    for (int i = 0; i < n; i++) NEG_(i) = (double)V_(i);
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++)
+        {
+            const double value = 1.0 * (PV_(pair_pos(i, j, n)) + 0.0) * dt;
+            if (fabs(value) >= DBL_EPSILON)
+            {
+                NEG_(i) += value;
+                NEG_(j) += -value;
+            }
+        }
+    const double hi_snap = 1.0 - p.eps_snap;
+    const double lo_snap = 0.0 + p.eps_snap;
+    double total = 0.0;
+    int m = 0;
+    for (int i = 0; i < n; i++)
+    {
+        double w = NEG_(i);
+        bool erase = false;
+        if (w >= hi_snap) w = 1.0;
+        if (w <= lo_snap) { w = 0.0; erase = true; }
+        total += w;
+        if (!erase)
+        {
+            G_(m) = G_(i);
+            NEG_(m) = w;
+            m++;
+        }
+    }
+    if (m > 1)
+    {
+        const double norm = 1.0 / total;
+        for (int i = 0; i < m; i++) V_(i) = (R)(NEG_(i) * norm);
+    }
+    else if (m == 1)
+    {
+        V_(0) = R(1);
+    }
+    else
+    {
+        st |= kStEmptyVoxel;
+    }
+    for (int i = 0; i < m; i++)
+        if (!isfinite((double)V_(i))) st |= kStNonFinite;
+#undef G_
+#undef V_
+#undef L_
+#undef SG_
+#undef PV_
+#undef POS_
+#undef NEG_
+    return m;
+}
+
+// One voxel of the step, reading its 3x3x3 neighbourhood straight from global memory, with its
+// working arrays in local memory (capacity KL fields).  This is the general path: the full-grid
+// kernel below and the overflow kernel of the tiled step (lists longer than the tiled kernel's
+// capacity) both run it.
+template <class R, int KS, int KL>
+__device__ __forceinline__ void voxel_step_generic(const StepParams& p, const StepArrays& a, long long v,
+                                                   int* s_key, double* s_sum, int nslots, unsigned& wide,
+                                                   unsigned& ein, unsigned& eout, uint32_t& st, bool count_in)
+{
+    const long long N = p.n;
+    const uint8_t* __restrict__ cnt = a.cnt_in;
+    const int16_t* __restrict__ gin = a.idx_in;
+    const R* __restrict__ vin = static_cast<const R*>(a.val_in);
+    R* __restrict__ vout = static_cast<R*>(a.val_out);
+
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int z = (int)(v % nz);
+    const long long t = v / nz;
+    const int y = (int)(t % ny);
+    const int x = (int)(t / ny);
+    const long long plane = (long long)ny * nz;
+    long long X[3], Y[3], Z[3];
+    X[0] = (long long)(x == 0 ? nx - 1 : x - 1) * plane; X[1] = (long long)x * plane;
+    X[2] = (long long)(x == nx - 1 ? 0 : x + 1) * plane;
+    Y[0] = (long long)(y == 0 ? ny - 1 : y - 1) * nz; Y[1] = (long long)y * nz;
+    Y[2] = (long long)(y == ny - 1 ? 0 : y + 1) * nz;
+    Z[0] = (z == 0 ? nz - 1 : z - 1); Z[1] = z; Z[2] = (z == nz - 1 ? 0 : z + 1);
+
+    const int c = cnt[v];
+    if (count_in) ein = c;
+    int flag = c > 1 ? 2 : 0;
+    if (flag == 0)
+    {
+        for (int q = 0; q < 27 && flag == 0; q++)
+        {
+            const long long u = X[q / 9] + Y[(q / 3) % 3] + Z[q % 3];
+            if (cnt[u] > 1) flag = 1;
+        }
+    }
+
+    if (flag == 0)
+    {
+        // bulk voxel: the state is carried over unchanged (no stage touches it)
+        a.cnt_out[v] = (uint8_t)c;
+        for (int s = 0; s < c; s++)
+        {
+            const int g = gin[s * N + v];
+            const R phi = vin[s * N + v];
+            a.idx_out[s * N + v] = (int16_t)g;
+            vout[s * N + v] = phi;
+            vol_insert_n(s_key, s_sum, nslots, a.vol_acc, g, (double)phi);
+        }
+        eout = c;
+        return;
+    }
+    wide = 1;
+    // ---- 1. own fields, then candidates, with Laplacians (stencil order) ------------------------
+    constexpr int KP = KL * (KL - 1) / 2;
+    int16_t gL[KL];
+    R val[KL], lap[KL], sg[KP];
+    double pv[KP], pos[KL], neg[KL];
+    int n = 0;
+    for (int s = 0; s < c; s++)
+    {
+        gL[n] = gin[s * N + v];
+        val[n] = vin[s * N + v];
+        lap[n] = R(0);
+        n++;
+    }
+    for (int q = 0; q < p.ns; q++)
+    {
+        const long long u = X[p.lap_d[q][0] + 1] + Y[p.lap_d[q][1] + 1] + Z[p.lap_d[q][2] + 1];
+        const R w = (R)p.lap_w[q];
+        const int cu = cnt[u];
+        for (int s = 0; s < cu; s++)
+        {
+            const R phi = vin[s * N + u];
+            if (phi != R(0))
+            {
+                const int g = gin[s * N + u];
+                const R l = w * phi;
+                int f = 0;
+                while (f < n && gL[f] != g) f++;
+                if (f < n) lap[f] += l;
+                else if (n < KL) { gL[n] = (int16_t)g; val[n] = R(0); lap[n] = l; n++; }
+                else st |= kStOverflowList;
+            }
+        }
+    }
+    // the gradient pass of CalculateDerivativesSR appends indices it meets first
+    for (int q = 0; q < p.ng; q++)
+    {
+        const long long u = X[p.grad_d[q][0] + 1] + Y[p.grad_d[q][1] + 1] + Z[p.grad_d[q][2] + 1];
+        const int cu = cnt[u];
+        for (int s = 0; s < cu; s++)
+        {
+            const R phi = vin[s * N + u];
+            if (phi != R(0))
+            {
+                const int g = gin[s * N + u];
+                int f = 0;
+                while (f < n && gL[f] != g) f++;
+                if (f == n)
+                {
+                    if (n < KL) { gL[n] = (int16_t)g; val[n] = R(0); lap[n] = R(0); n++; }
+                    else st |= kStOverflowList;
+                }
+            }
+        }
+    }
+    const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1};
+    int m = list_step<R>(p, a, sc, n, flag, st);
+    if (m > KS) { st |= kStOverflowK; m = KS; }
+    a.cnt_out[v] = (uint8_t)m;
+    for (int i = 0; i < m; i++)
+    {
+        a.idx_out[i * N + v] = gL[i];
+        vout[i * N + v] = val[i];
+        vol_insert_n(s_key, s_sum, nslots, a.vol_acc, gL[i], (double)val[i]);
+    }
+    eout = m;
+}
+
+// Per-block totals of the counters and the grain-volume table, flushed to global memory.
+__device__ __forceinline__ void flush_block(const StepArrays& a, unsigned wide, unsigned ein, unsigned eout,
+                                            uint32_t st, unsigned long long* s_cnt, const int* keys,
+                                            const double* sums, int nslots, int t, int nt)
+{
+    if (st) atomicOr(a.status, st);
+    unsigned w = wide, ei = ein, eo = eout;
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        w += __shfl_down_sync(0xffffffffu, w, o);
+        ei += __shfl_down_sync(0xffffffffu, ei, o);
+        eo += __shfl_down_sync(0xffffffffu, eo, o);
+    }
+    if ((t & 31) == 0)
+    {
+        if (w) atomicAdd(&s_cnt[0], (unsigned long long)w);
+        if (ei) atomicAdd(&s_cnt[1], (unsigned long long)ei);
+        if (eo) atomicAdd(&s_cnt[2], (unsigned long long)eo);
+    }
+    if (st & (kStOverflowK | kStOverflowList)) atomicAdd(&a.counters[kCntOverflowVoxels], 1ull);
+    __syncthreads();
+    for (int i = t; i < nslots; i += nt)
+        if (keys[i] >= 0) atomicAdd(&a.vol_acc[keys[i]], sums[i]);
+    if (t < 3 && s_cnt[t])
+        atomicAdd(&a.counters[t == 0 ? kCntWide : (t == 1 ? kCntEntriesIn : kCntEntriesOut)], s_cnt[t]);
 }
 
 template <class R, int KS, int KL>
@@ -437,30 +510,8 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned wide = 0, ein = 0, eout = 0;
     uint32_t st = 0;
-    if (v < p.n) voxel_step_generic<R, KS, KL>(p, a, v, s_key, s_sum, wide, ein, eout, st, true);
-
-    if (st) atomicOr(a.status, st);
-    // block totals of the counters
-    unsigned w = wide, ei = ein, eo = eout;
-    for (int o = 16; o > 0; o >>= 1)
-    {
-        w += __shfl_down_sync(0xffffffffu, w, o);
-        ei += __shfl_down_sync(0xffffffffu, ei, o);
-        eo += __shfl_down_sync(0xffffffffu, eo, o);
-    }
-    if ((threadIdx.x & 31) == 0)
-    {
-        if (w) atomicAdd(&s_cnt[0], (unsigned long long)w);
-        if (ei) atomicAdd(&s_cnt[1], (unsigned long long)ei);
-        if (eo) atomicAdd(&s_cnt[2], (unsigned long long)eo);
-    }
-    if (st & (kStOverflowK | kStOverflowList)) atomicAdd(&a.counters[kCntOverflowVoxels], 1ull);
-    __syncthreads();
-    for (int i = threadIdx.x; i < kVolSlots; i += blockDim.x)
-        if (s_key[i] >= 0) atomicAdd(&a.vol_acc[s_key[i]], s_sum[i]);
-    if (threadIdx.x < 3 && s_cnt[threadIdx.x])
-        atomicAdd(&a.counters[threadIdx.x == 0 ? kCntWide : (threadIdx.x == 1 ? kCntEntriesIn : kCntEntriesOut)],
-                  s_cnt[threadIdx.x]);
+    if (v < p.n) voxel_step_generic<R, KS, KL>(p, a, v, s_key, s_sum, kVolSlots, wide, ein, eout, st, true);
+    flush_block(a, wide, ein, eout, st, s_cnt, s_key, s_sum, kVolSlots, threadIdx.x, blockDim.x);
 }
 
 template <class R>
