@@ -93,7 +93,7 @@ struct StepArrays {
     int slice;                 // entries per classify-block slice
 };
 
-constexpr int kListCap = 6;    // list capacity of the split kernels (longer lists: overflow worklist)
+constexpr int kListCap = 8;    // list capacity of the split kernels (longer lists: overflow worklist)
 constexpr int kTileRows = 4;   // tile rows of the classify kernel (tiles of 32 x kTileRows voxels)
 
 // Launch geometry of the classify kernel: tiles of 32 (z) x kTileRows (y) voxels marching over

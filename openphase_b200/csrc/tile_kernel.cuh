@@ -620,7 +620,10 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream)
     list_compute_kernel<R, 4, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 5, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 6, KS><<<nblocks, 128, 0, s>>>(p, a);
-    overflow_step_kernel<R, KS, KL><<<148 * 2, 128, 0, s>>>(p, a);
+    list_compute_kernel<R, 7, KS><<<nblocks, 128, 0, s>>>(p, a);
+    list_compute_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a);
+    // one warp per SM: the general path's per-thread working arrays then stay in L1
+    overflow_step_kernel<R, KS, KL><<<148, 32, 0, s>>>(p, a);
     return (int)cudaGetLastError();
 }
 
