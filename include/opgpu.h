@@ -88,6 +88,9 @@ typedef struct opgpu_stats {
     uint32_t overflow_voxels;      /* voxels that raised OPGPU_E_OVERFLOW_K / _LIST               */
     int64_t timed_launches;        /* step-kernel launches timed since opgpu_set_timing(ctx, 1)     */
     double  timed_kernel_ms;       /* their summed device duration (CUDA events around each launch) */
+    int64_t general_path_total;    /* voxels processed by the general per-voxel path (long lists,
+                                      windows with too many grains) summed over all steps          */
+    int64_t crowded_window_total;  /* of those, voxels whose 3-plane window held too many grains  */
 } opgpu_stats;
 
 /* ---- lifecycle ------------------------------------------------------------------------------ */

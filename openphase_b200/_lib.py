@@ -64,7 +64,8 @@ class Stats(C.Structure):
     _fields_ = [("steps", C.c_int64), ("wide_last", C.c_int64), ("wide_total", C.c_int64),
                 ("entries_in_total", C.c_int64), ("entries_out_total", C.c_int64),
                 ("status", C.c_uint32), ("overflow_voxels", C.c_uint32), ("timed_launches", C.c_int64),
-                ("timed_kernel_ms", C.c_double)]
+                ("timed_kernel_ms", C.c_double), ("general_path_total", C.c_int64),
+                ("crowded_window_total", C.c_int64)]
 
 
 _lib = None

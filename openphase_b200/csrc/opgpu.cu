@@ -43,11 +43,9 @@ struct opgpu_ctx {
     int* d_slow_list = nullptr;      // overflow worklist of the tiled kernel (capacity N)
     unsigned* d_slow_count = nullptr;
     // work buffer of the classify / compute split (see tile_kernel.cuh)
-    void* d_wl_val = nullptr;
-    void* d_wl_lap = nullptr;
-    int16_t* d_wl_g = nullptr;
-    uint8_t* d_wl_flag = nullptr;
-    int* d_bucket = nullptr;
+    unsigned char* d_wl = nullptr;
+    long long wl_slice = 0;
+    int2* d_bucket = nullptr;
     unsigned* d_bucket_count = nullptr;
     long long bucket_cap = 0;
     int slice = 0;
@@ -174,6 +172,10 @@ __global__ void grains_update_kernel(int G, double* vol_acc, double* volume, dou
         counters[kCntEntriesOutTotal] += counters[kCntEntriesOut];
         counters[kCntWideLast] = counters[kCntWide];
         counters[kCntSteps] += 1;
+        counters[kCntGeneralTotal] += counters[kCntGeneralLast];
+        counters[kCntGeneralLast] = 0;
+        counters[kCntCrowdedTotal] += counters[kCntCrowdedLast];
+        counters[kCntCrowdedLast] = 0;
         counters[kCntWide] = 0;
         counters[kCntEntriesIn] = 0;
         counters[kCntEntriesOut] = 0;
@@ -393,11 +395,8 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
         const long long nblocks = (long long)gz * gy * gx;
         ctx->slice = 32 * kTileRows * xchunk;
         ctx->bucket_cap = nblocks * ctx->slice;
-        const size_t nl = (size_t)kListCap * ctx->n;
-        if (cudaMalloc(&ctx->d_wl_val, nl * ctx->rsz + 16) != cudaSuccess) return bail(OPGPU_E_CUDA);
-        if (cudaMalloc(&ctx->d_wl_lap, nl * ctx->rsz + 16) != cudaSuccess) return bail(OPGPU_E_CUDA);
-        if (dalloc(&ctx->d_wl_g, nl) != cudaSuccess) return bail(OPGPU_E_CUDA);
-        if (dalloc(&ctx->d_wl_flag, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        ctx->wl_slice = (long long)ctx->slice * work_record_bytes(kListCap, (int)ctx->rsz);
+        if (dalloc(&ctx->d_wl, (size_t)(nblocks * ctx->wl_slice)) != cudaSuccess) return bail(OPGPU_E_CUDA);
         if (dalloc(&ctx->d_bucket, (size_t)(kListCap + 1) * ctx->bucket_cap) != cudaSuccess) return bail(OPGPU_E_CUDA);
         if (dalloc(&ctx->d_bucket_count, (size_t)(kListCap + 1) * nblocks) != cudaSuccess) return bail(OPGPU_E_CUDA);
         if (cudaMemset(ctx->d_bucket_count, 0, (kListCap + 1) * nblocks * sizeof(unsigned)) != cudaSuccess)
@@ -433,7 +432,7 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     dfree(ctx->d_slow_list);
     dfree(ctx->d_slow_count);
-    dfree(ctx->d_wl_val); dfree(ctx->d_wl_lap); dfree(ctx->d_wl_g); dfree(ctx->d_wl_flag);
+    dfree(ctx->d_wl);
     dfree(ctx->d_bucket); dfree(ctx->d_bucket_count);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
@@ -677,7 +676,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
         a.dg_pair = pair_table ? ctx->d_dg_pair : nullptr;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
-        a.wl_val = ctx->d_wl_val; a.wl_lap = ctx->d_wl_lap; a.wl_g = ctx->d_wl_g; a.wl_flag = ctx->d_wl_flag;
+        a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
         a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
         a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;
         if (ctx->timing)
@@ -859,6 +858,8 @@ extern "C" uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats)
     stats->entries_out_total = (int64_t)c[kCntEntriesOutTotal];
     stats->status = ctx->status;
     stats->overflow_voxels = (uint32_t)c[kCntOverflowVoxels];
+    stats->general_path_total = (int64_t)c[kCntGeneralTotal];
+    stats->crowded_window_total = (int64_t)c[kCntCrowdedTotal];
     stats->timed_launches = ctx->timed_launches;
     stats->timed_kernel_ms = ctx->timed_ms;
     return OPGPU_OK;

@@ -30,8 +30,15 @@ enum : uint32_t {
 enum {
     kCntWide = 0, kCntEntriesIn = 1, kCntEntriesOut = 2, kCntOverflowVoxels = 3,
     kCntWideTotal = 4, kCntEntriesInTotal = 5, kCntEntriesOutTotal = 6, kCntWideLast = 7, kCntSteps = 8,
-    kNumCounters = 9
+    kCntGeneralLast = 9,      // voxels the last step sent through the general per-voxel path
+    kCntGeneralTotal = 10,
+    kCntCrowdedLast = 11,     // of those, voxels whose window held more grains than slots
+    kCntCrowdedTotal = 12,
+    kNumCounters = 13
 };
+
+// Bytes of a work-list record with n fields of type R: grains padded to 8 bytes, values, Laplacians.
+__host__ __device__ constexpr int work_record_bytes(int n, int rsz) { return ((2 * n + 7) / 8) * 8 + 2 * n * rsz; }
 
 struct StepParams {
     int nx, ny, nz;
@@ -82,12 +89,12 @@ struct StepArrays {
     int* slow_list;            // [slow_cap]
     unsigned* slow_count;      // reset by the launcher before every step
     unsigned slow_cap;
-    // work buffer between the classify kernel and the per-length compute kernels
-    void* wl_val;              // [kListCap][N] values of the list fields (own fields, then candidates)
-    void* wl_lap;              // [kListCap][N] their Laplacians
-    int16_t* wl_g;             // [kListCap][N] their grains
-    uint8_t* wl_flag;          // [N] interface flag of the voxel (1 or 2)
-    int* bucket;               // [kListCap + 1][bucket_cap] voxels per list length, block-private slices
+    // work buffer between the classify kernel and the per-length compute kernels: every list is a
+    // record of n fields (int16 grains padded to 8 bytes, then n values, then n Laplacians) packed
+    // in its classify block's byte slice; bucket entries (voxel | flag2 << 31, record offset)
+    unsigned char* wl;         // [blocks][wl_slice] bytes
+    long long wl_slice;        // bytes per classify block
+    int2* bucket;              // [kListCap + 1][bucket_cap] entries per list length, block-private slices
     unsigned* bucket_count;    // [kListCap + 1][max blocks] entries per slice
     long long bucket_cap;
     int slice;                 // entries per classify-block slice

@@ -28,6 +28,7 @@ namespace opgpu {
 
 constexpr int kTileZ = 32;
 constexpr int kSlots = 16;           // distinct grains per 3-plane window
+constexpr int kSlotHash = 64;        // grain -> slot hash table entries
 constexpr int kTileVolSlots = 512;
 constexpr int kTileTY = kTileRows;   // tile rows (blocks of 32 x kTileRows threads)
 
@@ -44,28 +45,59 @@ struct TileSmem {
     using Geo = TileGeom<TY>;
     R dense[kSlots][3][Geo::kRecs];          // per-slot values of the three ring planes
     double vol_sum[kTileVolSlots];
-    uint32_t mask[3][Geo::kRecs];            // slot bitmask per record
+    uint32_t word[3][Geo::kRecs];            // slot bitmask of the record | (more than one field) << 31
     int vol_key[kTileVolSlots];
     int grain_of[kSlots];                    // slot -> grain (-1 = free)
     int lastpos[kSlots];                     // last window position where the slot's grain occurs
+    int hkey[kSlotHash];                     // grain -> slot hash: key (-1 empty, -2 deleted)
     int pending[32];                         // grains of the incoming plane that need a slot
     unsigned nb[kListCap + 1];               // entries this block appended per list length
+    unsigned woff;                           // bytes of work records this block wrote
+    unsigned crowded;                        // voxels sent to the general path for a crowded window
     unsigned long long cnt[3];
+    uint8_t hslot[kSlotHash];                // grain -> slot hash: slot
     uint8_t slot[3][KS][Geo::kRecs];         // slot ids in entry order
     uint8_t cntr[3][Geo::kRecs];             // entries per record
     uint8_t bad[3];                          // ring plane holds a grain without slot
+    uint8_t tomb;                            // deleted hash entries
 };
 
-// Slot of a grain in the window table (-1 if absent).
-__device__ __forceinline__ int find_slot(const int* grain_of, int g)
+__device__ __forceinline__ unsigned slot_hash(int g) { return ((unsigned)g * 2654435761u) >> 26; }
+
+// Slot of a grain in the window (-1 if the grain has none).
+__device__ __forceinline__ int find_slot(const int* hkey, const uint8_t* hslot, int g)
 {
-    int r = -1;
-#pragma unroll
-    for (int k = 0; k < kSlots; k++) r = (grain_of[k] == g) ? k : r;
-    return r;
+    unsigned h = slot_hash(g);
+    for (int probe = 0; probe < kSlotHash; probe++)
+    {
+        const int k = hkey[h];
+        if (k == g) return hslot[h];
+        if (k == -1) return -1;
+        h = (h + 1) & (kSlotHash - 1);
+    }
+    return -1;
 }
 
-// Bring plane xp (window position wpos) into ring slot `rs`: slot lists, bitmasks and dense
+__device__ __forceinline__ void hash_insert(int* hkey, uint8_t* hslot, int g, int slot)
+{
+    unsigned h = slot_hash(g);
+    while (hkey[h] >= 0) h = (h + 1) & (kSlotHash - 1);
+    hkey[h] = g;
+    hslot[h] = (uint8_t)slot;
+}
+
+__device__ __forceinline__ void hash_erase(int* hkey, int g, uint8_t& tomb)
+{
+    unsigned h = slot_hash(g);
+    for (int probe = 0; probe < kSlotHash; probe++)
+    {
+        if (hkey[h] == g) { hkey[h] = -2; tomb++; return; }
+        if (hkey[h] == -1) return;
+        h = (h + 1) & (kSlotHash - 1);
+    }
+}
+
+// Bring plane xp (window position wpos) into ring slot `rs`: slot lists, bitmask words and dense
 // per-slot values.  Grains not yet in the window get a slot that no grain of the window uses.
 template <class R, int KS, int TY>
 __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
@@ -86,7 +118,7 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         for (int s = 0; s < c; s++)
         {
             const int g = a.idx_in[s * N + v];
-            if (find_slot(S.grain_of, g) < 0)
+            if (find_slot(S.hkey, S.hslot, g) < 0)
             {
                 unsigned h = ((unsigned)g * 2654435761u) & 31u;
                 for (int probe = 0; probe < 32; probe++)
@@ -99,7 +131,8 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         }
     }
     __syncthreads();
-    // 2. warp 0 hands free slots (grain gone from the window) to the pending grains
+    // 2. warp 0 hands free slots (grain gone from the window) to the pending grains; lane 0 keeps
+    //    the grain -> slot hash in step
     if (t < 32)
     {
         const int g = S.pending[t];
@@ -108,26 +141,37 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         const unsigned fm = __ballot_sync(0xffffffffu, is_free);
         const unsigned vm = __ballot_sync(0xffffffffu, valid);
         const int rank = __popc(vm & ((1u << t) - 1u));
-        bool fail = false;
-        if (valid)
+        const int k = (valid && rank < __popc(fm)) ? __fns(fm, 0, rank + 1) : -1;
+        if (valid) S.pending[t] = -1;
+        const unsigned fb = __ballot_sync(0xffffffffu, valid && k < 0);
+        for (int lane = 0; lane < 32; lane++)
         {
-            S.pending[t] = -1;
-            if (rank < __popc(fm))
+            if (!((vm >> lane) & 1u)) continue;
+            const int gl = __shfl_sync(0xffffffffu, g, lane);
+            const int kl = __shfl_sync(0xffffffffu, k, lane);
+            if (t == 0 && kl >= 0)
             {
-                const int k = __fns(fm, 0, rank + 1);
-                S.grain_of[k] = g;
-                S.lastpos[k] = wpos;
-            }
-            else
-            {
-                fail = true;
+                const int old = S.grain_of[kl];
+                if (old >= 0) hash_erase(S.hkey, old, S.tomb);
+                hash_insert(S.hkey, S.hslot, gl, kl);
+                S.grain_of[kl] = gl;
+                S.lastpos[kl] = wpos;
             }
         }
-        const unsigned fb = __ballot_sync(0xffffffffu, fail);
-        if (t == 0) S.bad[rs] = fb ? 1 : 0;
+        if (t == 0)
+        {
+            S.bad[rs] = fb ? 1 : 0;
+            if (S.tomb > 24)
+            {
+                for (int h = 0; h < kSlotHash; h++) S.hkey[h] = -1;
+                for (int q = 0; q < kSlots; q++)
+                    if (S.grain_of[q] >= 0) hash_insert(S.hkey, S.hslot, S.grain_of[q], q);
+                S.tomb = 0;
+            }
+        }
     }
     __syncthreads();
-    // 3. slot lists, bitmasks, dense values of the incoming plane
+    // 3. slot lists, bitmask words, dense values of the incoming plane
     for (int r = t; r < Geo::kRecs; r += Geo::NT)
     {
         const int row = r / Geo::kCols, col = r - row * Geo::kCols;
@@ -141,14 +185,14 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         for (int s = 0; s < c; s++)
         {
             const int g = a.idx_in[s * N + v];
-            const int k = find_slot(S.grain_of, g);
+            const int k = find_slot(S.hkey, S.hslot, g);
             if (k < 0) { S.bad[rs] = 1; continue; }
             S.dense[k][rs][r] = vin[s * N + v];
             S.slot[rs][s][r] = (uint8_t)k;
             msk |= 1u << k;
             S.lastpos[k] = wpos;
         }
-        S.mask[rs][r] = msk;
+        S.word[rs][r] = msk | (c > 1 ? 0x80000000u : 0u);
         S.cntr[rs][r] = (uint8_t)c;
     }
 }
@@ -162,6 +206,23 @@ __device__ __forceinline__ constexpr int stencil_dy(int q) { return NS == 27 ? (
 template <int NS>
 __device__ __forceinline__ constexpr int stencil_dz(int q) { return NS == 27 ? q % 3 - 1 : (q == 2 ? -1 : (q == 4 ? 1 : 0)); }
 
+// New grains of neighbour record (pl, r): append them in the record's entry order.
+template <class R, int KS, int TY>
+__device__ __forceinline__ void append_fresh(const TileSmem<R, KS, TY>& S, int pl, int r, uint32_t fresh,
+                                             uint8_t* ls, int& n, bool& over)
+{
+    const int cu = S.cntr[pl][r];
+    for (int s = 0; s < cu; s++)
+    {
+        const int k = S.slot[pl][s][r];
+        if ((fresh >> k) & 1u)
+        {
+            if (n < kListCap) ls[n++] = (uint8_t)k;
+            else over = true;
+        }
+    }
+}
+
 template <class R, int KS, int TY, int NS>
 __global__ void __launch_bounds__(32 * TY)
 tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, int xchunk)
@@ -169,6 +230,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     using Geo = TileGeom<TY>;
     using Smem = TileSmem<R, KS, TY>;
     constexpr int NT = Geo::NT;
+    constexpr int kC = Geo::kCols;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
 
@@ -181,16 +243,18 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     const int z = z0 + tz, y = y0 + ty;
     const bool inside = (z < nz) && (y < ny);
     const int blin = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    const long long nblocks = (long long)gridDim.x * gridDim.y * gridDim.z;
     const long long slice0 = (long long)blin * a.slice;
+    unsigned char* __restrict__ wbase = a.wl + (long long)blin * a.wl_slice;
     R* __restrict__ vout = static_cast<R*>(a.val_out);
-    R* __restrict__ wval = static_cast<R*>(a.wl_val);
-    R* __restrict__ wlap = static_cast<R*>(a.wl_lap);
 
     for (int i = t; i < kTileVolSlots; i += NT) { S.vol_key[i] = -1; S.vol_sum[i] = 0.0; }
     if (t < kSlots) { S.grain_of[t] = -1; S.lastpos[t] = -1000; }
+    if (t < kSlotHash) S.hkey[t] = -1;
     if (t < 32) S.pending[t] = -1;
     if (t <= kListCap) S.nb[t] = 0u;
     if (t < 3) S.cnt[t] = 0ull;
+    if (t == 0) { S.woff = 0u; S.crowded = 0u; S.tomb = 0; }
     unsigned wide = 0, ein = 0, eout = 0;
     uint32_t st = 0;
     __syncthreads();
@@ -198,7 +262,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     load_plane(p, a, S, 0, x0 == 0 ? nx - 1 : x0 - 1, -1, y0, z0, t);
     __syncthreads();
     load_plane(p, a, S, 1, x0, 0, y0, z0, t);
-    const int rec0 = (ty + 1) * Geo::kCols + (tz + 1);
+    const int rec0 = (ty + 1) * kC + (tz + 1);
 
     for (int x = x0; x < x1; x++)
     {
@@ -213,17 +277,29 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
 
         const int c = S.cntr[sl1][rec0];
         ein += c;
-        int flag = c > 1 ? 2 : 0;
-        if (flag == 0)
-        {
+        // ---- flag and (27-point stencils) candidate discovery in one pass over the neighbours ----
+        uint8_t ls[kListCap];
+        int n = c;
+        bool over = window_bad || c > kListCap;
+        if (!over)
+            for (int k = 0; k < c; k++) ls[k] = S.slot[sl1][k][rec0];
+        uint32_t seen = S.word[sl1][rec0] & 0xFFFFu;
+        uint32_t multi = 0;
 #pragma unroll
-            for (int q = 0; q < 27; q++)
+        for (int q = 0; q < 27; q++)
+        {
+            const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
+            const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
+            const uint32_t w = S.word[pl][r];
+            multi |= w;
+            if (NS == 27 && q != 13)
             {
-                const int r = rec0 + ((q / 3) % 3 - 1) * Geo::kCols + (q % 3 - 1);
-                const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
-                if (S.cntr[pl][r] > 1) flag = 1;
+                const uint32_t fresh = w & 0xFFFFu & ~seen;
+                if (fresh && !over) append_fresh(S, pl, r, fresh, ls, n, over);
+                seen |= w & 0xFFFFu;
             }
         }
+        const int flag = c > 1 ? 2 : ((multi >> 31) ? 1 : 0);
         if (flag == 0)
         {
             // bulk voxel: carried over unchanged
@@ -240,45 +316,34 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
             continue;
         }
         wide++;
-        // ---- candidate discovery: own fields, then new grains in stencil / neighbour-list order ----
-        uint8_t ls[kListCap];
-        bool over = window_bad || c > kListCap;
-        int n = c;
-        if (!over)
+        if (NS != 27 && !over)
         {
-            for (int k = 0; k < c; k++) ls[k] = S.slot[sl1][k][rec0];
-            uint32_t seen = S.mask[sl1][rec0];
+            // 7-point Laplacian: its stencil order, then the gradient pass over the 26 neighbours
+            seen = S.word[sl1][rec0] & 0xFFFFu;
             const int nq = p.ns + p.ng;
             for (int q = 0; q < nq && !over; q++)
             {
                 const signed char* d = q < p.ns ? p.lap_d[q] : p.grad_d[q - p.ns];
                 const int pl = d[0] < 0 ? sl0 : (d[0] > 0 ? sl2 : sl1);
-                const int r = rec0 + d[1] * Geo::kCols + d[2];
-                const uint32_t fresh = S.mask[pl][r] & ~seen;
-                if (fresh)
-                {
-                    const int cu = S.cntr[pl][r];
-                    for (int s = 0; s < cu; s++)
-                    {
-                        const int k = S.slot[pl][s][r];
-                        if ((fresh >> k) & 1u)
-                        {
-                            if (n < kListCap) ls[n++] = (uint8_t)k;
-                            else over = true;
-                        }
-                    }
-                    seen |= fresh;
-                }
+                const int r = rec0 + d[1] * kC + d[2];
+                const uint32_t fresh = S.word[pl][r] & 0xFFFFu & ~seen;
+                if (fresh) append_fresh(S, pl, r, fresh, ls, n, over);
+                seen |= fresh;
             }
         }
         if (over || n < 2)
         {
+            if (window_bad) atomicAdd(&S.crowded, 1u);
             const unsigned slot = atomicAdd(a.slow_count, 1u);
             if (slot < a.slow_cap) a.slow_list[slot] = (int)v;
             else st |= kStOverflowList;
             continue;
         }
-        // ---- values and Laplacians from the dense planes into the work buffer ----------------------
+        // ---- values and Laplacians from the dense planes into a work record ----------------------
+        const int pad = ((2 * n + 7) / 8) * 8;
+        const unsigned off = atomicAdd(&S.woff, (unsigned)(pad + 2 * n * (int)sizeof(R)));
+        int16_t* rg = reinterpret_cast<int16_t*>(wbase + off);
+        R* rv = reinterpret_cast<R*>(wbase + off + pad);
         for (int k = 0; k < n; k++)
         {
             const int s = ls[k];
@@ -288,19 +353,20 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
             {
                 const int dx = stencil_dx<NS>(q);
                 const int pl = dx < 0 ? sl0 : (dx > 0 ? sl2 : sl1);
-                const int r = rec0 + stencil_dy<NS>(q) * Geo::kCols + stencil_dz<NS>(q);
+                const int r = rec0 + stencil_dy<NS>(q) * kC + stencil_dz<NS>(q);
                 l += (R)p.lap_w[q] * S.dense[s][pl][r];
             }
-            a.wl_g[k * N + v] = (int16_t)S.grain_of[s];
-            wval[k * N + v] = S.dense[s][sl1][rec0];
-            wlap[k * N + v] = l;
+            rg[k] = (int16_t)S.grain_of[s];
+            rv[k] = S.dense[s][sl1][rec0];
+            rv[n + k] = l;
         }
-        a.wl_flag[v] = (uint8_t)flag;
         const unsigned rank = atomicAdd(&S.nb[n], 1u);
-        a.bucket[(long long)n * a.bucket_cap + slice0 + rank] = (int)v;
+        a.bucket[(long long)n * a.bucket_cap + slice0 + rank] =
+            make_int2((int)v | (flag == 2 ? (int)0x80000000 : 0), (int)off);
     }
     __syncthreads();
-    if (t >= 2 && t <= kListCap) a.bucket_count[t * (long long)(gridDim.x * gridDim.y * gridDim.z) + blin] = S.nb[t];
+    if (t >= 2 && t <= kListCap) a.bucket_count[t * nblocks + blin] = S.nb[t];
+    if (t == 0 && S.crowded) atomicAdd(&a.counters[kCntCrowdedLast], (unsigned long long)S.crowded);
     flush_block(a, wide, ein, eout, st, S.cnt, S.vol_key, S.vol_sum, kTileVolSlots, t, NT);
 }
 
@@ -320,24 +386,27 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     if (t < 3) s_cnt[t] = 0ull;
     __syncthreads();
     const long long N_ = p.n;
-    const int* __restrict__ list = a.bucket + (long long)N * a.bucket_cap + (long long)blockIdx.x * a.slice;
-    const R* __restrict__ wval = static_cast<const R*>(a.wl_val);
-    const R* __restrict__ wlap = static_cast<const R*>(a.wl_lap);
+    const int2* __restrict__ list = a.bucket + (long long)N * a.bucket_cap + (long long)blockIdx.x * a.slice;
+    const unsigned char* __restrict__ wbase = a.wl + (long long)blockIdx.x * a.wl_slice;
+    constexpr int kPad = ((2 * N + 7) / 8) * 8;
     R* __restrict__ vout = static_cast<R*>(a.val_out);
     uint32_t st = 0;
     unsigned eout = 0;
     for (unsigned e = t; e < cnt; e += blockDim.x)
     {
-        const long long v = list[e];
-        const int flag = a.wl_flag[v];
+        const int2 ent = list[e];
+        const long long v = ent.x & 0x7fffffff;
+        const int flag = (ent.x >> 31) ? 2 : 1;
+        const int16_t* __restrict__ rg = reinterpret_cast<const int16_t*>(wbase + ent.y);
+        const R* __restrict__ rv = reinterpret_cast<const R*>(wbase + ent.y + kPad);
         int g[N];
         R val[N], lap[N];
 #pragma unroll
         for (int k = 0; k < N; k++)
         {
-            g[k] = a.wl_g[k * N_ + v];
-            val[k] = wval[k * N_ + v];
-            lap[k] = wlap[k * N_ + v];
+            g[k] = rg[k];
+            val[k] = rv[k];
+            lap[k] = rv[N + k];
         }
         // ---- pair kinetics ---------------------------------------------------------------------
         double localN;
@@ -589,6 +658,7 @@ __global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constan
     if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0ull;
     __syncthreads();
     const unsigned total = min(*a.slow_count, a.slow_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters[kCntGeneralLast], (unsigned long long)total);
     uint32_t st = 0;
     unsigned eo_sum = 0;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
