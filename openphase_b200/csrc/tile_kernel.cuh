@@ -118,7 +118,12 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         for (int s = 0; s < c; s++)
         {
             const int g = a.idx_in[s * N + v];
-            if (find_slot(S.hkey, S.hslot, g) < 0)
+            const int k0 = find_slot(S.hkey, S.hslot, g);
+            if (k0 >= 0)
+            {
+                S.lastpos[k0] = wpos;   // in use by the incoming plane: not free for step 2
+            }
+            else
             {
                 unsigned h = ((unsigned)g * 2654435761u) & 31u;
                 for (int probe = 0; probe < 32; probe++)

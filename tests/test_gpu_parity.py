@@ -19,11 +19,16 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-9
 
-# grains larger than the reference volume 4/3*pi*iwidth^3: VolumeRatio = 1 throughout
+# every grain far above the reference volume 4/3*pi*iwidth^3 (VolumeRatio = 1 throughout) and no
+# driving force (no tanh): bit-identical to the oracle over long runs
 STRICT = {
-    "lb_16": Case(16, 16, 16, 6, seed=3, iwidth=4.0, dt=0.1, name="lb_16"),
-    "isotropic": Case(24, 20, 16, 10, seed=5, iwidth=5.0, dt=0.1, stencil="ISOTROPIC", name="isotropic"),
-    "simple": Case(24, 20, 16, 10, seed=5, iwidth=5.0, dt=0.1, stencil="SIMPLE", name="simple"),
+    "lb_big": Case(40, 40, 32, 8, seed=3, iwidth=4.0, dt=0.1, name="lb_big"),
+    "isotropic_big": Case(48, 40, 32, 8, seed=5, iwidth=5.0, dt=0.1, stencil="ISOTROPIC", name="isotropic_big"),
+    "simple_big": Case(48, 40, 32, 8, seed=6, iwidth=5.0, dt=0.1, stencil="SIMPLE", name="simple_big"),
+}
+# per-grain-pair sigma and driving force with large grains: tanh differs between CUDA and libm in the
+# last bits, so the bar holds for 60 steps and borderline decisions are counted after that
+DRIVEN = {
     "pairs_dg_48": Case(48, 40, 32, 12, seed=8, iwidth=5.0, dt=0.08, sigma=1.2, sigma_pairs=(0.8, 0.4),
                         dg_scale=0.05, name="pairs_dg_48"),
 }
@@ -76,6 +81,22 @@ def test_fp64_matches_oracle_strict(name, variant):
     print(name, variant, res[-1])
 
 
+@pytest.mark.parametrize("name", list(DRIVEN))
+def test_fp64_matches_oracle_driven(name):
+    case = DRIVEN[name]
+    res = _run_pair(case, [1, 2, 10, 60, 150])
+    for s, r in res:
+        if s:
+            assert r["status_gpu"] & 0b11 == 0, (s, r)
+        if s <= 60:
+            assert r["non_borderline_mismatch_voxels"] == 0, (s, r)
+            assert r["max_dphi"] <= TOL, (s, r)
+        else:
+            assert r["set_mismatch_voxels"] <= 1e-4 * case.n, (s, r)
+            assert r["vol_rel"] <= 1e-9, (s, r)
+    print(name, res[-1])
+
+
 @pytest.mark.parametrize("name", list(SMALL))
 def test_fp64_matches_oracle_small_grains(name):
     case = SMALL[name]
@@ -107,7 +128,7 @@ def test_fp64_normal_grain_growth_64_1000_steps():
 
 
 def test_fp64_wide_interface_count_and_flags():
-    case = STRICT["pairs_dg_48"]
+    case = DRIVEN["pairs_dg_48"]
     state = case.initial_state()
     ora = Oracle(case, *state)
     ctx = Context.from_case(case, precision="fp64", k_slots=16, state=state)
@@ -120,13 +141,13 @@ def test_fp64_wide_interface_count_and_flags():
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("name", ["pairs_dg", "dg_strong", "simple"])
+@pytest.mark.parametrize("name", ["pairs_dg", "dg_strong", "simple_big"])
 def test_tiled_kernel_equals_generic_kernel(name, precision):
     """The tiled production kernels (shared-memory halo ring, per-length register kernels, overflow
     worklist for long lists) and the full-grid generic kernel run the same per-voxel arithmetic:
     identical index lists and values equal up to the last-bit effect of the grain-volume summation
     order (these small grains have VolumeRatio < 1, which feeds the volumes back)."""
-    case = (SMALL | STRICT)[name]
+    case = (SMALL | STRICT | DRIVEN)[name]
     state = case.initial_state()
     a = Context.from_case(case, precision=precision, k_slots=16, state=state)
     b = Context.from_case(case, precision=precision, k_slots=16, state=state)
