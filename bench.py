@@ -163,7 +163,8 @@ def device_run(case, precision, k_slots, steps, warmup, device, state, sigma, dg
     wide = s1["wide_total"] - s0["wide_total"]
     ctx.close()
     return {
-        "elapsed_ms": elapsed_ms, "kernel_ms": s1["timed_kernel_ms"], "kernel_launches": s1["timed_launches"],
+        "elapsed_ms": elapsed_ms, "kernel_ms": s1["timed_kernel_ms"], "timed_steps": s1["timed_launches"],
+        "classify_ms": s1["timed_classify_ms"], "gpu_launches": s1["kernel_launches"] - s0["kernel_launches"],
         "entries_in": entries_in, "entries_out": entries_out, "wide": wide, "status": status | s1["status"],
         "clocks": clk.summary(),
     }
@@ -322,19 +323,27 @@ def main():
         ms = agg(r["elapsed_ms"])
         s = 4 if precision == "fp32" else 8
         value = world * case.n * args.steps / (ms / 1e3)
-        launches = max(1, r["kernel_launches"])
-        kernel_ms = r["kernel_ms"] / launches
-        # algorithmic bytes of one step: every voxel's count byte and stored entries read once,
-        # the new count byte and entries written once
-        bytes_per_launch = 2 * case.n + (r["entries_in"] + r["entries_out"]) * (2 + s) / args.steps
+        nsteps_timed = max(1, r["timed_steps"])
+        kernel_ms = r["kernel_ms"] / nsteps_timed
+        classify_ms = r["classify_ms"] / nsteps_timed
+        # algorithmic bytes of one step (the K = 8 slot record of every wide-interface voxel read
+        # and written once, plus one count byte per voxel for the flag/worklist pass)
+        wide_per_step = r["wide"] / args.steps
+        bytes_per_launch = wide_per_step * 2 * (1 + 8 * (2 + s)) + case.n
+        # the same with only the stored entries counted (what the sparse slot layout moves)
+        sparse_bytes = 2 * case.n + (r["entries_in"] + r["entries_out"]) * (2 + s) / args.steps
         achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
         traffic = profiled_traffic(precision)
         out[precision] = {
             "value": value, "ms_per_step": ms / args.steps, "status": r["status"], "clocks": r["clocks"],
+            "gpu_launches": r["gpu_launches"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "step_kernel", "kernel_ms": kernel_ms,
+                         "kernel": "step: tile_classify_kernel + list_compute_kernel<N=2..8> + overflow_step_kernel",
+                         "kernel_ms": kernel_ms, "classify_ms": classify_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "sparse_bytes_per_launch": sparse_bytes,
+                         "sparse_achieved": sparse_bytes / (kernel_ms / 1e3) / 1e9,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s"},
             "wide_fraction": r["wide"] / (case.n * args.steps),
@@ -368,7 +377,7 @@ def main():
                    "initial_state_seconds": round(t_init, 2)},
         "clocks": f32["clocks"],
         "e2e": e2e,
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": f32["gpu_launches"],
         "roofline": f32["roofline"],
         "cpu_baseline": cpu,
         "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "roofline": f64["roofline"],

@@ -86,11 +86,14 @@ typedef struct opgpu_stats {
     int64_t entries_out_total;     /* sum over steps of stored entries written                    */
     uint32_t status;               /* OR of soft OPGPU_E_* bits since the last opgpu_clear_status  */
     uint32_t overflow_voxels;      /* voxels that raised OPGPU_E_OVERFLOW_K / _LIST               */
-    int64_t timed_launches;        /* step-kernel launches timed since opgpu_set_timing(ctx, 1)     */
-    double  timed_kernel_ms;       /* their summed device duration (CUDA events around each launch) */
+    int64_t timed_launches;        /* steps timed since opgpu_set_timing(ctx, 1)                   */
+    double  timed_kernel_ms;       /* their summed device duration: CUDA events on the context's
+                                      stream around each step's kernel sequence                    */
     int64_t general_path_total;    /* voxels processed by the general per-voxel path (long lists,
                                       windows with too many grains) summed over all steps          */
     int64_t crowded_window_total;  /* of those, voxels whose 3-plane window held too many grains  */
+    double  timed_classify_ms;     /* of timed_kernel_ms, the part spent in the classify kernel     */
+    int64_t kernel_launches;       /* kernels this library launched for steps since creation       */
 } opgpu_stats;
 
 /* ---- lifecycle ------------------------------------------------------------------------------ */

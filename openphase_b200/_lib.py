@@ -65,7 +65,8 @@ class Stats(C.Structure):
                 ("entries_in_total", C.c_int64), ("entries_out_total", C.c_int64),
                 ("status", C.c_uint32), ("overflow_voxels", C.c_uint32), ("timed_launches", C.c_int64),
                 ("timed_kernel_ms", C.c_double), ("general_path_total", C.c_int64),
-                ("crowded_window_total", C.c_int64)]
+                ("crowded_window_total", C.c_int64), ("timed_classify_ms", C.c_double),
+                ("kernel_launches", C.c_int64)]
 
 
 _lib = None

@@ -78,6 +78,13 @@ def grain_growth_dg_256() -> Case:
                 sigma_pairs=(0.8, 0.4), dg_scale=0.05, name="grain_growth_dg_256")
 
 
+def grain_growth_dg_128() -> Case:
+    """The 256^3 workload scaled to 128^3 at the same mean grain size (250 grains): the case the
+    kernel profiles are captured on."""
+    return Case(128, 128, 128, 250, seed=2, iwidth=6.0, dt=0.08, nsteps=2000, sigma=1.2, mu=1.0,
+                sigma_pairs=(0.8, 0.4), dg_scale=0.05, name="grain_growth_dg_128")
+
+
 def adjoint_calibration_128() -> Case:
     return Case(128, 128, 128, 256, seed=4, iwidth=5.0, dt=0.08, nsteps=200, sigma=1.2, mu=1.0,
                 sigma_pairs=(0.8, 0.4), dg_scale=0.03, name="adjoint_calibration_128")

@@ -54,12 +54,14 @@ struct opgpu_ctx {
     bool model_set = false, state_loaded = false, initialized = false;
     uint32_t status = 0;
     double nvf = 1.0;   // NucleusVolumeFactor
-    // per-launch timing of the step kernel
+    // per-step timing of the step kernels (events: start, after classify, end)
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
-    size_t ev_used = 0;          // event pairs recorded and not yet read
+    size_t ev_used = 0;          // event triples recorded and not yet read
     long long timed_launches = 0;
     double timed_ms = 0.0;
+    double timed_classify_ms = 0.0;
+    long long kernel_launches = 0;   // kernels of this library launched on the context's stream
 };
 
 namespace {
@@ -322,9 +324,11 @@ uint32_t read_status(opgpu_ctx* ctx)
     CK(cudaStreamSynchronize(ctx->stream));
     for (size_t i = 0; i < ctx->ev_used; i++)
     {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * i], ctx->ev_pool[2 * i + 1]));
+        float ms = 0.f, ms_c = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev_pool[3 * i], ctx->ev_pool[3 * i + 2]));
+        CK(cudaEventElapsedTime(&ms_c, ctx->ev_pool[3 * i], ctx->ev_pool[3 * i + 1]));
         ctx->timed_ms += ms;
+        ctx->timed_classify_ms += ms_c;
         ctx->timed_launches++;
     }
     ctx->ev_used = 0;
@@ -662,6 +666,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
     {
         if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, (size_t)ctx->G * ctx->G));
         const int rc = launch_dg_pair(sp, ctx->d_dg, ctx->d_gphase, ctx->d_dg_pair, ctx->stream);
+        ctx->kernel_launches++;
         if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("driving-force table: ") + cudaGetErrorString((cudaError_t)rc));
         ctx->dg_pair_dirty = false;
     }
@@ -679,27 +684,33 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
         a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
         a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
         a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;
+        LaunchInfo info;
         if (ctx->timing)
         {
-            if (ctx->ev_pool.size() < 2 * (ctx->ev_used + 1))
+            if (ctx->ev_pool.size() < 3 * (ctx->ev_used + 1))
             {
-                for (int k = 0; k < 2; k++)
+                for (int k = 0; k < 3; k++)
                 {
                     cudaEvent_t e;
                     CK(cudaEventCreate(&e));
                     ctx->ev_pool.push_back(e);
                 }
             }
-            CK(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], ctx->stream));
+            CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used], ctx->stream));
+            info.after_classify = ctx->ev_pool[3 * ctx->ev_used + 1];
         }
-        const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->variant, ctx->stream)
-                                 : launch_step_f64(sp, a, ctx->K, ctx->variant, ctx->stream);
+        const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->variant, ctx->stream, &info)
+                                 : launch_step_f64(sp, a, ctx->K, ctx->variant, ctx->stream, &info);
         if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("step launch: ") + cudaGetErrorString((cudaError_t)rc));
         if (ctx->timing)
         {
-            CK(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used + 1], ctx->stream));
+            // the generic variant has no classify phase: its "after classify" event is the start
+            if (ctx->variant == kVariantGeneric)
+                CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used + 1], ctx->stream));
+            CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used + 2], ctx->stream));
             ctx->ev_used++;
         }
+        ctx->kernel_launches += info.kernels + 1;   // + grains_update_kernel
         grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
             ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 1);
         CK(cudaGetLastError());
@@ -862,6 +873,8 @@ extern "C" uint32_t opgpu_get_stats(opgpu_ctx* ctx, opgpu_stats* stats)
     stats->crowded_window_total = (int64_t)c[kCntCrowdedTotal];
     stats->timed_launches = ctx->timed_launches;
     stats->timed_kernel_ms = ctx->timed_ms;
+    stats->timed_classify_ms = ctx->timed_classify_ms;
+    stats->kernel_launches = ctx->kernel_launches;
     return OPGPU_OK;
 }
 
@@ -883,6 +896,7 @@ extern "C" uint32_t opgpu_set_timing(opgpu_ctx* ctx, int32_t enable)
     {
         ctx->timed_launches = 0;
         ctx->timed_ms = 0.0;
+        ctx->timed_classify_ms = 0.0;
     }
     return OPGPU_OK;
 }

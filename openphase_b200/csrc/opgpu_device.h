@@ -119,10 +119,19 @@ inline void tiled_geometry(int nx, int ny, int nz, int* xchunk, int* gz, int* gy
 
 enum { kVariantTiled = 0, kVariantGeneric = 1 };
 
+// Filled by the launchers: kernels launched, and an event recorded after the classify kernel
+// (when `after_classify` is not null) so the caller can time it separately.
+struct LaunchInfo {
+    void* after_classify = nullptr;   // cudaEvent_t
+    int kernels = 0;
+};
+
 // Launchers (defined in step_f64.cu / step_f32.cu).  k_slots in {8, 12, 16}; variant selects the
 // tiled production kernel or the full-grid generic kernel (same results, used for validation).
-int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream);
-int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream);
+int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
+                    LaunchInfo* info);
+int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
+                    LaunchInfo* info);
 // Fill out[a*G+b] with the limited driving force of every grain pair (defined in step_f64.cu, so
 // that it is compiled exactly like the in-place evaluation of the FP64 form).
 int launch_dg_pair(const StepParams& p, const double* dg, const int16_t* gphase, double* out, void* stream);

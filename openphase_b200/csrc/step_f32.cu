@@ -3,8 +3,9 @@
 #include "tile_kernel.cuh"
 
 namespace opgpu {
-int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream)
+int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
+                    LaunchInfo* info)
 {
-    return launch_step<float>(p, a, k_slots, variant, stream);
+    return launch_step<float>(p, a, k_slots, variant, stream, info);
 }
 }  // namespace opgpu

@@ -4,9 +4,10 @@
 
 namespace opgpu {
 
-int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream)
+int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
+                    LaunchInfo* info)
 {
-    return launch_step<double>(p, a, k_slots, variant, stream);
+    return launch_step<double>(p, a, k_slots, variant, stream, info);
 }
 
 __global__ void dg_pair_kernel(const __grid_constant__ StepParams p, const double* __restrict__ dg,

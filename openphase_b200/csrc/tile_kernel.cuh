@@ -146,7 +146,7 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         const unsigned fm = __ballot_sync(0xffffffffu, is_free);
         const unsigned vm = __ballot_sync(0xffffffffu, valid);
         const int rank = __popc(vm & ((1u << t) - 1u));
-        const int k = (valid && rank < __popc(fm)) ? __fns(fm, 0, rank + 1) : -1;
+        const int k = (valid && rank < __popc(fm)) ? (int)__fns(fm, 0, rank + 1) : -1;
         if (valid) S.pending[t] = -1;
         const unsigned fb = __ballot_sync(0xffffffffu, valid && k < 0);
         for (int lane = 0; lane < 32; lane++)
@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constan
 }
 
 template <class R, int KS, int KL, int NS>
-int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream)
+int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, LaunchInfo* info)
 {
     using Smem = TileSmem<R, KS, kTileTY>;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -690,6 +690,11 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream)
     e = cudaMemsetAsync(a.slow_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return (int)e;
     kern<<<dim3(gz, gy, gx), dim3(32, kTileTY), smem, s>>>(p, a, xchunk);
+    if (info && info->after_classify)
+    {
+        e = cudaEventRecord(static_cast<cudaEvent_t>(info->after_classify), s);
+        if (e != cudaSuccess) return (int)e;
+    }
     list_compute_kernel<R, 2, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 3, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 4, KS><<<nblocks, 128, 0, s>>>(p, a);
@@ -699,26 +704,32 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream)
     list_compute_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a);
     // one warp per SM: the general path's per-thread working arrays then stay in L1
     overflow_step_kernel<R, KS, KL><<<148, 32, 0, s>>>(p, a);
+    if (info) info->kernels += 9;
     return (int)cudaGetLastError();
 }
 
 template <class R, int KS, int KL>
-int launch_tiled(const StepParams& p, const StepArrays& a, void* stream)
+int launch_tiled(const StepParams& p, const StepArrays& a, void* stream, LaunchInfo* info)
 {
-    if (p.ns == 27) return launch_tiled_ns<R, KS, KL, 27>(p, a, stream);
-    if (p.ns == 7) return launch_tiled_ns<R, KS, KL, 7>(p, a, stream);
+    if (p.ns == 27) return launch_tiled_ns<R, KS, KL, 27>(p, a, stream, info);
+    if (p.ns == 7) return launch_tiled_ns<R, KS, KL, 7>(p, a, stream, info);
     return -1;
 }
 
 template <class R>
-int launch_step(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream)
+int launch_step(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
+                LaunchInfo* info)
 {
-    if (variant == kVariantGeneric) return launch_step_generic<R>(p, a, k_slots, stream);
+    if (variant == kVariantGeneric)
+    {
+        if (info) info->kernels += 1;
+        return launch_step_generic<R>(p, a, k_slots, stream);
+    }
     switch (k_slots)
     {
-        case 8:  return launch_tiled<R, 8, 16>(p, a, stream);
-        case 12: return launch_tiled<R, 12, 20>(p, a, stream);
-        case 16: return launch_tiled<R, 16, 24>(p, a, stream);
+        case 8:  return launch_tiled<R, 8, 16>(p, a, stream, info);
+        case 12: return launch_tiled<R, 12, 20>(p, a, stream, info);
+        case 16: return launch_tiled<R, 16, 24>(p, a, stream, info);
         default: return -1;
     }
 }

@@ -18,6 +18,7 @@ def compare_states(a, b, ngrains, borderline=1e-12, eps_snap=np.finfo(np.float64
       borderline_voxels  mismatching voxels whose extra entries sit within `borderline` of the
                           finalize erase threshold in the engine that kept them
       max_dphi           max |phi_a - phi_b| over the union of entries (missing entries count as 0)
+      frac_over_1e4      fraction of the union entries with |phi_a - phi_b| > 1e-4
     """
     ca, ia, va = a
     cb, ib, vb = b
@@ -36,6 +37,7 @@ def compare_states(a, b, ngrains, borderline=1e-12, eps_snap=np.finfo(np.float64
     pa[ina] = va_s
     pb[inb] = vb_s
     out["max_dphi"] = float(np.max(np.abs(pa - pb))) if keys.size else 0.0
+    out["frac_over_1e4"] = float(np.count_nonzero(np.abs(pa - pb) > 1e-4)) / max(1, keys.size)
     only = ina ^ inb
     vox = keys[only] // ngrains
     out["set_mismatch_voxels"] = int(np.unique(vox).size)
