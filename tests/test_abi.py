@@ -124,3 +124,11 @@ def test_raw_format_round_trip(tmp_path):
     dims, c2, i2, v2 = init.parse_raw(data)
     assert dims == (1, 2, 2)
     assert np.array_equal(c2, counts) and np.array_equal(i2, idx) and np.array_equal(v2, val)
+
+
+def test_cxx_mirror_compiles_and_links(tmp_path):
+    """The C++ mirror of the reference classes (include/opgpu.hpp) builds into a NormalGG-shaped
+    caller linked against the in-tree library."""
+    from tests.cxx_build import build_normal_gg
+    exe = build_normal_gg(tmp_path)
+    assert exe.exists()
