@@ -143,6 +143,17 @@ uint32_t opgpu_download_lists(opgpu_ctx* ctx, int32_t* counts, int32_t* idx, dou
 /* Per-voxel flags (0 bulk, 1 interface halo, 2 interface) of the current state
  * (PhaseField::SetFlagsSR, src/PhaseField.cpp:953-969). */
 uint32_t opgpu_download_flags(opgpu_ctx* ctx, int8_t* flags);
+/* Same result as opgpu_download_flags, but the call allocates no device memory (no cudaMalloc /
+ * cudaFree, no allocating library routine): the flags are computed into a fixed 16 MiB scratch
+ * array in the library's device memory and copied from there.  No reference counterpart.
+ * For callers that cannot allocate: a host whose device memory is fully handed out to its own
+ * pool, and callers that must not stall other streams (cudaFree waits for all work on the
+ * device), e.g. a monitor that reads the flags while steps run on other contexts.
+ * Limit: grids of at most 16,777,216 voxels (256^3); larger grids get OPGPU_E_INVALID with a
+ * message.  The first call on a device does a one-time set-up (it looks up the scratch address
+ * on that device) and should come before any stream capture.  The scratch is shared by all
+ * contexts on a device: overlapping calls (from several threads) race, so serialise them. */
+uint32_t opgpu_download_flags_noalloc(opgpu_ctx* ctx, int8_t* flags);
 
 /* ---- the time step -------------------------------------------------------------------------- */
 /* nsteps repetitions of the reference step sequence

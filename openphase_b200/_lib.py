@@ -91,6 +91,7 @@ _SIGS = {
     "opgpu_total_entries": (C.c_uint32, [_P, C.POINTER(C.c_int64)]),
     "opgpu_download_lists": (C.c_uint32, [_P, _P, _P, _P]),
     "opgpu_download_flags": (C.c_uint32, [_P, _P]),
+    "opgpu_download_flags_noalloc": (C.c_uint32, [_P, _P]),
     "opgpu_step": (C.c_uint32, [_P, C.c_double, C.c_int32]),
     "opgpu_step_async": (C.c_uint32, [_P, C.c_double, C.c_int32]),
     "opgpu_sync": (C.c_uint32, [_P]),

@@ -126,6 +126,12 @@ class Context:
         _check(lib().opgpu_download_flags(self.h, ptr(f)), self.h, "download_flags")
         return f
 
+    def flags_noalloc(self):
+        """The flags through opgpu_download_flags_noalloc (no device allocation; grids up to 256^3)."""
+        f = np.empty(self.n, dtype=np.int8)
+        _check(lib().opgpu_download_flags_noalloc(self.h, ptr(f)), self.h, "download_flags_noalloc")
+        return f
+
     def grains(self):
         G = self.ngrains
         vol, vr, mx = (np.empty(G) for _ in range(3))

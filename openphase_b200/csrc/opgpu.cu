@@ -11,6 +11,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -811,6 +812,53 @@ extern "C" uint32_t opgpu_download_flags(opgpu_ctx* ctx, int8_t* flags)
     CK(cudaMemcpyAsync(flags, d_flags, N, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     dfree(d_flags);
+    return OPGPU_OK;
+}
+
+// ---- allocation-free flag download ------------------------------------------------------------
+// The flags are computed into a file-scope device array instead of a per-call cudaMalloc'd
+// buffer.  Its address is looked up once per device (cudaGetSymbolAddress, with that device
+// current) and cached.  Every one of the N bytes is written by flags_kernel before the copy, so
+// nothing in the scratch has to start at zero.  The scratch is shared by every context on a
+// device: overlapping calls race.
+namespace {
+constexpr long long kNoAllocFlagsMax = 16LL << 20;   // bytes = voxels (a 256^3 grid)
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) int8_t g_noalloc_flags[kNoAllocFlagsMax];
+std::mutex g_noalloc_mu;
+int8_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+extern "C" uint32_t opgpu_download_flags_noalloc(opgpu_ctx* ctx, int8_t* flags)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    if (!flags) return fail(ctx, OPGPU_E_INVALID, "opgpu_download_flags_noalloc: flags is NULL");
+    if (ctx->n > kNoAllocFlagsMax)
+        return fail(ctx, OPGPU_E_INVALID,
+                    "opgpu_download_flags_noalloc: grid of " + std::to_string(ctx->n) +
+                    " voxels exceeds its fixed scratch of 16777216 voxels; use opgpu_download_flags");
+    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
+        return fail(ctx, OPGPU_E_INVALID, "opgpu_download_flags_noalloc: device ordinal above 63");
+    if (!ctx->state_loaded) return fail(ctx, OPGPU_E_STATE, "no state");
+    int8_t* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[ctx->device])
+        {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_flags);
+            if (e != cudaSuccess)
+                return fail(ctx, OPGPU_E_CUDA, std::string("opgpu_download_flags_noalloc: set-up: ") + cudaGetErrorString(e));
+            g_noalloc_ptr[ctx->device] = static_cast<int8_t*>(p);
+        }
+        scratch = g_noalloc_ptr[ctx->device];
+    }
+    const long long N = ctx->n;
+    flags_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(ctx->grid.nx, ctx->grid.ny, ctx->grid.nz,
+                                                             ctx->cnt[ctx->cur], scratch);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(flags, scratch, N, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return OPGPU_OK;
 }
 
