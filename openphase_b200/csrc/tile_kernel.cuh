@@ -29,7 +29,8 @@ namespace opgpu {
 constexpr int kTileZ = 32;
 constexpr int kSlots = 16;           // distinct grains per 3-plane window
 constexpr int kSlotHash = 64;        // grain -> slot hash table entries
-constexpr int kTileVolSlots = 512;
+constexpr int kTileVolSlots = 512;      // grain-volume hash of the compute kernels
+constexpr int kClassifyVolSlots = 256;  // grain-volume hash of the classify kernel (bulk voxels)
 constexpr int kTileTY = kTileRows;   // tile rows (blocks of 32 x kTileRows threads)
 
 template <int TY>
@@ -43,10 +44,11 @@ struct TileGeom {
 template <class R, int KS, int TY>
 struct TileSmem {
     using Geo = TileGeom<TY>;
-    R dense[kSlots][3][Geo::kRecs];          // per-slot values of the three ring planes
-    double vol_sum[kTileVolSlots];
+    R dense[kSlots][3][Geo::kRecs];          // per-slot values of the three ring planes (zero where absent)
+    double vol_sum[kClassifyVolSlots];
+    uint64_t slotl[3][Geo::kRecs];           // slot ids of the record in entry order, 4 bits each
     uint32_t word[3][Geo::kRecs];            // slot bitmask of the record | (more than one field) << 31
-    int vol_key[kTileVolSlots];
+    int vol_key[kClassifyVolSlots];
     int grain_of[kSlots];                    // slot -> grain (-1 = free)
     int lastpos[kSlots];                     // last window position where the slot's grain occurs
     int hkey[kSlotHash];                     // grain -> slot hash: key (-1 empty, -2 deleted)
@@ -56,7 +58,6 @@ struct TileSmem {
     unsigned crowded;                        // voxels sent to the general path for a crowded window
     unsigned long long cnt[3];
     uint8_t hslot[kSlotHash];                // grain -> slot hash: slot
-    uint8_t slot[3][KS][Geo::kRecs];         // slot ids in entry order
     uint8_t cntr[3][Geo::kRecs];             // entries per record
     uint8_t bad[3];                          // ring plane holds a grain without slot
     uint8_t tomb;                            // deleted hash entries
@@ -81,9 +82,11 @@ __device__ __forceinline__ int find_slot(const int* hkey, const uint8_t* hslot, 
 __device__ __forceinline__ void hash_insert(int* hkey, uint8_t* hslot, int g, int slot)
 {
     unsigned h = slot_hash(g);
-    while (hkey[h] >= 0) h = (h + 1) & (kSlotHash - 1);
-    hkey[h] = g;
-    hslot[h] = (uint8_t)slot;
+    for (int probe = 0; probe < kSlotHash; probe++)
+    {
+        if (hkey[h] < 0) { hkey[h] = g; hslot[h] = (uint8_t)slot; return; }
+        h = (h + 1) & (kSlotHash - 1);
+    }
 }
 
 __device__ __forceinline__ void hash_erase(int* hkey, int g, uint8_t& tomb)
@@ -97,27 +100,83 @@ __device__ __forceinline__ void hash_erase(int* hkey, int g, uint8_t& tomb)
     }
 }
 
-// Bring plane xp (window position wpos) into ring slot `rs`: slot lists, bitmask words and dense
-// per-slot values.  Grains not yet in the window get a slot that no grain of the window uses.
-template <class R, int KS, int TY>
-__device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
-                                           int rs, int xp, int wpos, int y0, int z0, int t)
+// Records of a ring plane each thread handles, and how many entries of each it keeps in registers
+// between the two passes of load_plane.
+template <int TY>
+struct PlaneRegs {
+    static constexpr int kPer = (TileGeom<TY>::kRecs + TileGeom<TY>::NT - 1) / TileGeom<TY>::NT;
+    static constexpr int kKeep = 6;
+};
+
+template <int TY>
+__device__ __forceinline__ long long plane_voxel(const StepParams& p, long long base, int r, int y0, int z0)
 {
     using Geo = TileGeom<TY>;
+    const int row = r / Geo::kCols, col = r - row * Geo::kCols;
+    int yy = y0 - 1 + row; yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy % p.ny : yy);
+    int zz = z0 - 1 + col; zz = zz < 0 ? zz + p.nz : (zz >= p.nz ? zz % p.nz : zz);
+    return base + (long long)yy * p.nz + zz;
+}
+
+// Counts of plane xp for this thread's records (issued one plane ahead of their use).
+template <int TY>
+__device__ __forceinline__ void prefetch_counts(const StepParams& p, const StepArrays& a, int xp, int y0, int z0,
+                                                int t, int (&cr)[PlaneRegs<TY>::kPer])
+{
+    using Geo = TileGeom<TY>;
+    const long long base = (long long)xp * p.ny * p.nz;
+#pragma unroll
+    for (int i = 0; i < PlaneRegs<TY>::kPer; i++)
+    {
+        const int r = t + i * Geo::NT;
+        cr[i] = r < Geo::kRecs ? (int)a.cnt_in[plane_voxel<TY>(p, base, r, y0, z0)] : 0;
+    }
+}
+
+// Bring plane xp (window position wpos) into ring slot `rs`: slot lists, bitmask words and dense
+// per-slot values.  Grains not yet in the window get a slot that no grain of the window uses.
+// cr holds the plane's counts on entry (prefetched) and the next plane's counts on return.
+// Invariant of the dense planes: dense[k][rs][r] != 0 only if bit k of word[rs][r] is set.
+template <class R, int KS, int TY>
+__device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
+                                           int rs, int xp, int wpos, int y0, int z0, int t,
+                                           int (&cr)[PlaneRegs<TY>::kPer])
+{
+    using Geo = TileGeom<TY>;
+    using PR = PlaneRegs<TY>;
     const long long N = p.n;
     const long long base = (long long)xp * p.ny * p.nz;
     const R* __restrict__ vin = static_cast<const R*>(a.val_in);
-    // 1. grains of the incoming plane without a slot
-    for (int r = t; r < Geo::kRecs; r += Geo::NT)
+    long long vv[PR::kPer];
+    int gr[PR::kPer][PR::kKeep];
+    R vr[PR::kPer][PR::kKeep];
+    // 1. read the records once (the first kKeep entries stay in registers); mark the grains already
+    //    slotted as in use, collect the others in `pending`
+#pragma unroll
+    for (int i = 0; i < PR::kPer; i++)
     {
-        const int row = r / Geo::kCols, col = r - row * Geo::kCols;
-        int yy = y0 - 1 + row; yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy % p.ny : yy);
-        int zz = z0 - 1 + col; zz = zz < 0 ? zz + p.nz : (zz >= p.nz ? zz % p.nz : zz);
-        const long long v = base + (long long)yy * p.nz + zz;
-        const int c = a.cnt_in[v];
-        for (int s = 0; s < c; s++)
+        const int r = t + i * Geo::NT;
+        vv[i] = r < Geo::kRecs ? plane_voxel<TY>(p, base, r, y0, z0) : 0;
+#pragma unroll
+        for (int s = 0; s < PR::kKeep; s++)
         {
-            const int g = a.idx_in[s * N + v];
+            if (s < cr[i])
+            {
+                gr[i][s] = a.idx_in[s * N + vv[i]];
+                vr[i][s] = vin[s * N + vv[i]];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < PR::kPer; i++)
+    {
+        for (int s = 0; s < cr[i]; s++)
+        {
+            int g;
+#pragma unroll
+            for (int q = 0; q < PR::kKeep; q++)
+                if (q == s) g = gr[i][q];
+            if (s >= PR::kKeep) g = a.idx_in[s * N + vv[i]];
             const int k0 = find_slot(S.hkey, S.hslot, g);
             if (k0 >= 0)
             {
@@ -149,9 +208,9 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         const int k = (valid && rank < __popc(fm)) ? (int)__fns(fm, 0, rank + 1) : -1;
         if (valid) S.pending[t] = -1;
         const unsigned fb = __ballot_sync(0xffffffffu, valid && k < 0);
-        for (int lane = 0; lane < 32; lane++)
+        for (unsigned m = vm; m; m &= m - 1u)
         {
-            if (!((vm >> lane) & 1u)) continue;
+            const int lane = __ffs(m) - 1;
             const int gl = __shfl_sync(0xffffffffu, g, lane);
             const int kl = __shfl_sync(0xffffffffu, k, lane);
             if (t == 0 && kl >= 0)
@@ -176,30 +235,38 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         }
     }
     __syncthreads();
-    // 3. slot lists, bitmask words, dense values of the incoming plane
-    for (int r = t; r < Geo::kRecs; r += Geo::NT)
-    {
-        const int row = r / Geo::kCols, col = r - row * Geo::kCols;
-        int yy = y0 - 1 + row; yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy % p.ny : yy);
-        int zz = z0 - 1 + col; zz = zz < 0 ? zz + p.nz : (zz >= p.nz ? zz % p.nz : zz);
-        const long long v = base + (long long)yy * p.nz + zz;
-        const int c = a.cnt_in[v];
+    // 3. slot lists, bitmask words, dense values of the incoming plane (clearing what the ring
+    //    position held before)
 #pragma unroll
-        for (int k = 0; k < kSlots; k++) S.dense[k][rs][r] = R(0);
+    for (int i = 0; i < PR::kPer; i++)
+    {
+        const int r = t + i * Geo::NT;
+        if (r >= Geo::kRecs) continue;
+        for (uint32_t m = S.word[rs][r] & 0xFFFFu; m; m &= m - 1u) S.dense[__ffs(m) - 1][rs][r] = R(0);
         uint32_t msk = 0;
+        uint64_t lst = 0;
+        const int c = cr[i];
         for (int s = 0; s < c; s++)
         {
-            const int g = a.idx_in[s * N + v];
+            int g;
+            R val;
+#pragma unroll
+            for (int q = 0; q < PR::kKeep; q++)
+                if (q == s) { g = gr[i][q]; val = vr[i][q]; }
+            if (s >= PR::kKeep) { g = a.idx_in[s * N + vv[i]]; val = vin[s * N + vv[i]]; }
             const int k = find_slot(S.hkey, S.hslot, g);
             if (k < 0) { S.bad[rs] = 1; continue; }
-            S.dense[k][rs][r] = vin[s * N + v];
-            S.slot[rs][s][r] = (uint8_t)k;
+            S.dense[k][rs][r] = val;
+            lst |= (uint64_t)k << (4 * s);
             msk |= 1u << k;
             S.lastpos[k] = wpos;
         }
         S.word[rs][r] = msk | (c > 1 ? 0x80000000u : 0u);
+        S.slotl[rs][r] = lst;
         S.cntr[rs][r] = (uint8_t)c;
     }
+    // counts of the next plane, for the next call
+    prefetch_counts<TY>(p, a, xp == p.nx - 1 ? 0 : xp + 1, y0, z0, t, cr);
 }
 
 // Offsets of the q-th Laplacian stencil element (LaplacianStencil::Set order): 27-point stencils
@@ -211,18 +278,19 @@ __device__ __forceinline__ constexpr int stencil_dy(int q) { return NS == 27 ? (
 template <int NS>
 __device__ __forceinline__ constexpr int stencil_dz(int q) { return NS == 27 ? q % 3 - 1 : (q == 2 ? -1 : (q == 4 ? 1 : 0)); }
 
-// New grains of neighbour record (pl, r): append them in the record's entry order.
+// New grains of neighbour record (pl, r): append them (4-bit slot ids) in the record's entry order.
 template <class R, int KS, int TY>
 __device__ __forceinline__ void append_fresh(const TileSmem<R, KS, TY>& S, int pl, int r, uint32_t fresh,
-                                             uint8_t* ls, int& n, bool& over)
+                                             uint64_t& ls, int& n, bool& over)
 {
     const int cu = S.cntr[pl][r];
-    for (int s = 0; s < cu; s++)
+    uint64_t lst = S.slotl[pl][r];
+    for (int s = 0; s < cu; s++, lst >>= 4)
     {
-        const int k = S.slot[pl][s][r];
+        const int k = (int)(lst & 15u);
         if ((fresh >> k) & 1u)
         {
-            if (n < kListCap) ls[n++] = (uint8_t)k;
+            if (n < kListCap) { ls |= (uint64_t)k << (4 * n); n++; }
             else over = true;
         }
     }
@@ -253,7 +321,9 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     unsigned char* __restrict__ wbase = a.wl + (long long)blin * a.wl_slice;
     R* __restrict__ vout = static_cast<R*>(a.val_out);
 
-    for (int i = t; i < kTileVolSlots; i += NT) { S.vol_key[i] = -1; S.vol_sum[i] = 0.0; }
+    for (int i = t; i < kClassifyVolSlots; i += NT) { S.vol_key[i] = -1; S.vol_sum[i] = 0.0; }
+    for (int i = t; i < kSlots * 3 * Geo::kRecs; i += NT) (&S.dense[0][0][0])[i] = R(0);
+    for (int i = t; i < 3 * Geo::kRecs; i += NT) (&S.word[0][0])[i] = 0u;
     if (t < kSlots) { S.grain_of[t] = -1; S.lastpos[t] = -1000; }
     if (t < kSlotHash) S.hkey[t] = -1;
     if (t < 32) S.pending[t] = -1;
@@ -262,11 +332,13 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     if (t == 0) { S.woff = 0u; S.crowded = 0u; S.tomb = 0; }
     unsigned wide = 0, ein = 0, eout = 0;
     uint32_t st = 0;
+    int cr[PlaneRegs<TY>::kPer];
+    prefetch_counts<TY>(p, a, x0 == 0 ? nx - 1 : x0 - 1, y0, z0, t, cr);
     __syncthreads();
 
-    load_plane(p, a, S, 0, x0 == 0 ? nx - 1 : x0 - 1, -1, y0, z0, t);
+    load_plane(p, a, S, 0, x0 == 0 ? nx - 1 : x0 - 1, -1, y0, z0, t, cr);
     __syncthreads();
-    load_plane(p, a, S, 1, x0, 0, y0, z0, t);
+    load_plane(p, a, S, 1, x0, 0, y0, z0, t, cr);
     const int rec0 = (ty + 1) * kC + (tz + 1);
 
     for (int x = x0; x < x1; x++)
@@ -274,7 +346,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         const int xi = x - x0;
         const int sl0 = xi % 3, sl1 = (xi + 1) % 3, sl2 = (xi + 2) % 3;
         __syncthreads();
-        load_plane(p, a, S, sl2, x == nx - 1 ? 0 : x + 1, xi + 1, y0, z0, t);
+        load_plane(p, a, S, sl2, x == nx - 1 ? 0 : x + 1, xi + 1, y0, z0, t, cr);
         __syncthreads();
         if (!inside) continue;
         const bool window_bad = S.bad[0] | S.bad[1] | S.bad[2];
@@ -283,11 +355,10 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         const int c = S.cntr[sl1][rec0];
         ein += c;
         // ---- flag and (27-point stencils) candidate discovery in one pass over the neighbours ----
-        uint8_t ls[kListCap];
+        uint64_t ls = 0;
         int n = c;
         bool over = window_bad || c > kListCap;
-        if (!over)
-            for (int k = 0; k < c; k++) ls[k] = S.slot[sl1][k][rec0];
+        if (!over) ls = S.slotl[sl1][rec0];   // c <= kListCap entries, unused nibbles are zero
         uint32_t seen = S.word[sl1][rec0] & 0xFFFFu;
         uint32_t multi = 0;
 #pragma unroll
@@ -315,7 +386,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
                 const R phi = static_cast<const R*>(a.val_in)[s * N + v];
                 a.idx_out[s * N + v] = (int16_t)g;
                 vout[s * N + v] = phi;
-                vol_insert_n(S.vol_key, S.vol_sum, kTileVolSlots, a.vol_acc, g, (double)phi);
+                vol_insert_n(S.vol_key, S.vol_sum, kClassifyVolSlots, a.vol_acc, g, (double)phi);
             }
             eout += c;
             continue;
@@ -351,7 +422,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         R* rv = reinterpret_cast<R*>(wbase + off + pad);
         for (int k = 0; k < n; k++)
         {
-            const int s = ls[k];
+            const int s = (int)((ls >> (4 * k)) & 15u);
             R l = R(0);
 #pragma unroll
             for (int q = 0; q < NS; q++)
@@ -372,7 +443,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     __syncthreads();
     if (t >= 2 && t <= kListCap) a.bucket_count[t * nblocks + blin] = S.nb[t];
     if (t == 0 && S.crowded) atomicAdd(&a.counters[kCntCrowdedLast], (unsigned long long)S.crowded);
-    flush_block(a, wide, ein, eout, st, S.cnt, S.vol_key, S.vol_sum, kTileVolSlots, t, NT);
+    flush_block(a, wide, ein, eout, st, S.cnt, S.vol_key, S.vol_sum, kClassifyVolSlots, t, NT);
 }
 
 // Stages 2-5 for lists of exactly N fields (compile-time), all arrays in registers; the operation
