@@ -204,6 +204,39 @@ def e2e_run(case, precision, k_slots, steps, device, state, sigma, dg):
     return {"seconds": t1 - t0, "h2d_per_step": h2d / steps, "d2h_per_step": d2h / steps}
 
 
+def adjoint_run(device):
+    """Cost of the checkpointed adjoint against the forward on the calibration rollout: 128^3,
+    256 grains, FP32 states, 200 steps, checkpoints every 16 steps, loss sum_g (V_g(T) - V*_g)^2."""
+    import torch
+    from openphase_b200.adjoint import Rollout
+    from openphase_b200.cases import adjoint_calibration_128
+    from openphase_b200.context import Context
+
+    case = adjoint_calibration_128()
+    G = case.ngrains
+    state = case.initial_state()
+    ctx = Context.from_case(case, precision="fp32", k_slots=16, device=device, state=state)
+    mu = np.ones((G, G))
+    R = Rollout(ctx, case.dt, case.nsteps, interval=16)
+    R.set_parameters(case.pair_sigma(), mu, case.driving_force())
+    target = R.forward()
+    R.set_parameters(np.full((G, G), 1.0), mu, np.zeros(G))
+    R.forward()                                   # warm-up of both passes
+    R.backward(np.ones(G))
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    V = R.forward()
+    torch.cuda.synchronize(device)
+    t1 = time.perf_counter()
+    R.backward(2.0 * (V - target))
+    torch.cuda.synchronize(device)
+    t2 = time.perf_counter()
+    ctx.close()
+    return {"workload": case.name, "steps": case.nsteps, "checkpoint_interval": 16, "dtype": "f32 states, f64 adjoint",
+            "forward_ms": 1e3 * (t1 - t0), "adjoint_ms": 1e3 * (t2 - t1), "adjoint_over_forward": (t2 - t1) / (t1 - t0),
+            "status": int(R.adjoint_status)}
+
+
 def reference_steps(case, state, warmup, steps, threads):
     """Time the reference's own CPU implementation (oracle/_ref, built from the reference sources)
     on the host cores: returns per-step seconds of the timed steps and the thread count."""
@@ -279,6 +312,7 @@ def main():
     ap.add_argument("--k-slots", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--workload", default="grain_growth_dg_256")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -356,6 +390,10 @@ def main():
         e2e = {"value": world * case.n * args.steps / sec, "unit": UNIT,
                "h2d_bytes_per_step": int(er["h2d_per_step"]), "d2h_bytes_per_step": int(er["d2h_per_step"])}
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_run(local_rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, state, os.cpu_count() or 1)
@@ -383,6 +421,7 @@ def main():
         "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "roofline": f64["roofline"],
                  "clocks": f64["clocks"], "status": f64["status"]},
         "fp32_over_fp64": f32["value"] / f64["value"],
+        "adjoint": adjoint,
         "status": {"fp32": f32["status"], "fp64": f64["status"]},
         "wide_fraction": f32["wide_fraction"],
     }

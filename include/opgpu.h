@@ -34,6 +34,7 @@ extern "C" {
 #define OPGPU_E_NORMALIZE_WARN  (1u << 3)  /* NormalizeIncrements plausibility warning                */
 #define OPGPU_E_LIMITER_CAP     (1u << 4)  /* increment limiter stopped after its 25 iterations       */
 #define OPGPU_E_NONFINITE       (1u << 5)  /* a non-finite phase-field value was produced             */
+#define OPGPU_E_ADJOINT_MISMATCH (1u << 6) /* adjoint step: recomputed step differs from the stored one */
 /* hard errors */
 #define OPGPU_E_INVALID         (1u << 8)  /* invalid argument                                         */
 #define OPGPU_E_CUDA            (1u << 9)  /* CUDA runtime error (message: opgpu_last_error)           */
@@ -183,6 +184,38 @@ uint32_t opgpu_set_timing(opgpu_ctx* ctx, int32_t enable);
 uint32_t opgpu_clear_status(opgpu_ctx* ctx);
 /* CUDA stream of the context (a cudaStream_t), for callers that order their own work after it. */
 void*    opgpu_stream(opgpu_ctx* ctx);
+
+/* ---- checkpoints, adjoint and tangent-linear model ------------------------------------------ */
+/* None of these has a reference counterpart: OpenPhase has no adjoint.  Parameters are the
+ * per-grain-pair interface energy sigma(a,b) and mobility mu(a,b) the step uses (symmetric G*G
+ * tables, diagonal unused) and the per-grain driving force dG(g); the loss is any function of the
+ * grain volumes V(g) of the current state.  The discrete decisions of each step (list members,
+ * zeroed and limited increments, snapped and erased fields) are those of the forward run and held
+ * fixed; VolumeRatio is held fixed.  Both precisions record states; the adjoint arithmetic and the
+ * gradient accumulation are FP64.  The tangent-linear model runs the FP64 form. */
+/* Reserve nslots device checkpoints (state plus grain records). */
+uint32_t opgpu_checkpoint_reserve(opgpu_ctx* ctx, int32_t nslots);
+/* Copy the current state and grain records into / out of a checkpoint slot. */
+uint32_t opgpu_checkpoint_save(opgpu_ctx* ctx, int32_t slot);
+uint32_t opgpu_checkpoint_load(opgpu_ctx* ctx, int32_t slot);
+/* Start a reverse sweep at the current state: the adjoint of every stored value is dL_dV[grain]
+ * (dL_dV[G]); the gradient accumulators are zeroed. */
+uint32_t opgpu_adjoint_begin(opgpu_ctx* ctx, const double* dL_dV);
+/* One step backwards.  `slot` holds the state from which one forward step of length dt produced the
+ * current state.  Accumulates the parameter gradients of that step, turns the adjoint into that of
+ * the slot's state and makes the slot's state current.  OPGPU_E_* bit 6 is raised when the
+ * recomputed step does not reproduce the current state's lists. */
+uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt);
+/* Accumulated gradients: dL_dsigma[G*G], dL_dmu[G*G] (symmetric, zero diagonal), dL_ddG[G]; any may
+ * be NULL. */
+uint32_t opgpu_adjoint_gradients(opgpu_ctx* ctx, double* dL_dsigma, double* dL_dmu, double* dL_ddG);
+/* Tangent-linear model: parameter tangents (symmetric G*G tables, G values; NULL = zero); the
+ * tangent of the current state starts at zero. */
+uint32_t opgpu_tlm_begin(opgpu_ctx* ctx, const double* dsigma, const double* dmu, const double* ddG);
+/* nsteps forward steps carrying the tangent (FP64 form; the state advances exactly as opgpu_step's). */
+uint32_t opgpu_tlm_step(opgpu_ctx* ctx, double dt, int32_t nsteps);
+/* Tangent of the grain volumes of the current state, dV[G]. */
+uint32_t opgpu_tlm_volumes(opgpu_ctx* ctx, double* dV);
 
 /* ---- host-side initial states (no GPU needed) ---------------------------------------------- */
 /* Counter-based generator shared by host and device: SplitMix64 (Steele, Lea, Flood 2014) over

@@ -19,6 +19,7 @@ E_EMPTY_VOXEL = 1 << 2
 E_NORMALIZE_WARN = 1 << 3
 E_LIMITER_CAP = 1 << 4
 E_NONFINITE = 1 << 5
+E_ADJOINT_MISMATCH = 1 << 6
 E_INVALID = 1 << 8
 E_CUDA = 1 << 9
 E_IO = 1 << 10
@@ -33,6 +34,7 @@ STAGE_STABLE, STAGE_SEED, STAGE_NUCLEUS = 0, 1, 2
 _CODE_NAMES = {
     E_OVERFLOW_K: "OVERFLOW_K", E_OVERFLOW_LIST: "OVERFLOW_LIST", E_EMPTY_VOXEL: "EMPTY_VOXEL",
     E_NORMALIZE_WARN: "NORMALIZE_WARN", E_LIMITER_CAP: "LIMITER_CAP", E_NONFINITE: "NONFINITE",
+    E_ADJOINT_MISMATCH: "ADJOINT_MISMATCH",
     E_INVALID: "INVALID", E_CUDA: "CUDA", E_IO: "IO", E_STATE: "STATE", E_NODEVICE: "NODEVICE",
 }
 
@@ -101,6 +103,15 @@ _SIGS = {
     "opgpu_set_timing": (C.c_uint32, [_P, C.c_int32]),
     "opgpu_set_kernel_variant": (C.c_uint32, [_P, C.c_int32]),
     "opgpu_stream": (_P, [_P]),
+    "opgpu_checkpoint_reserve": (C.c_uint32, [_P, C.c_int32]),
+    "opgpu_checkpoint_save": (C.c_uint32, [_P, C.c_int32]),
+    "opgpu_checkpoint_load": (C.c_uint32, [_P, C.c_int32]),
+    "opgpu_adjoint_begin": (C.c_uint32, [_P, _P]),
+    "opgpu_adjoint_step": (C.c_uint32, [_P, C.c_int32, C.c_double]),
+    "opgpu_adjoint_gradients": (C.c_uint32, [_P, _P, _P, _P]),
+    "opgpu_tlm_begin": (C.c_uint32, [_P, _P, _P, _P]),
+    "opgpu_tlm_step": (C.c_uint32, [_P, C.c_double, C.c_int32]),
+    "opgpu_tlm_volumes": (C.c_uint32, [_P, _P]),
     "opgpu_uniform": (C.c_double, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
     "opgpu_voronoi_owner_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                               C.c_int32, _P]),

@@ -29,6 +29,7 @@ CU_UNITS = {
     "opgpu.cu": [],
     "step_f64.cu": ["--fmad=false"],
     "step_f32.cu": ["--fmad=true"],
+    "adjoint.cu": ["--fmad=false"],
 }
 CPP_UNITS = ["host_init.cpp"]
 

@@ -159,6 +159,42 @@ class Context:
     def stream(self) -> int:
         return lib().opgpu_stream(self.h) or 0
 
+    # ---- checkpoints, adjoint, tangent-linear model
+    def checkpoint_reserve(self, nslots: int):
+        _check(lib().opgpu_checkpoint_reserve(self.h, int(nslots)), self.h, "checkpoint_reserve")
+
+    def checkpoint_save(self, slot: int):
+        _check(lib().opgpu_checkpoint_save(self.h, int(slot)), self.h, "checkpoint_save")
+
+    def checkpoint_load(self, slot: int):
+        _check(lib().opgpu_checkpoint_load(self.h, int(slot)), self.h, "checkpoint_load")
+
+    def adjoint_begin(self, dL_dV):
+        w = np.ascontiguousarray(dL_dV, dtype=np.float64)
+        _check(lib().opgpu_adjoint_begin(self.h, ptr(w)), self.h, "adjoint_begin")
+
+    def adjoint_step(self, slot: int, dt: float) -> int:
+        return _check(lib().opgpu_adjoint_step(self.h, int(slot), float(dt)), self.h, "adjoint_step")
+
+    def adjoint_gradients(self):
+        G = self.ngrains
+        ds, dm, dd = np.empty((G, G)), np.empty((G, G)), np.empty(G)
+        _check(lib().opgpu_adjoint_gradients(self.h, ptr(ds), ptr(dm), ptr(dd)), self.h, "adjoint_gradients")
+        return ds, dm, dd
+
+    def tlm_begin(self, dsigma=None, dmu=None, ddg=None):
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        ds, dm, dd = conv(dsigma), conv(dmu), conv(ddg)
+        _check(lib().opgpu_tlm_begin(self.h, ptr(ds), ptr(dm), ptr(dd)), self.h, "tlm_begin")
+
+    def tlm_step(self, dt: float, nsteps: int = 1) -> int:
+        return _check(lib().opgpu_tlm_step(self.h, float(dt), int(nsteps)), self.h, "tlm_step")
+
+    def tlm_volumes(self):
+        dV = np.empty(self.ngrains)
+        _check(lib().opgpu_tlm_volumes(self.h, ptr(dV)), self.h, "tlm_volumes")
+        return dV
+
     # ---- convenience
     @classmethod
     def from_case(cls, case, precision="fp64", k_slots=8, device=0, state=None, threads=0):

@@ -1,6 +1,7 @@
 // opgpu context: device memory, parameter tables, state upload/download, grain records and the
 // step loop of the C ABI declared in include/opgpu.h.
 #include "opgpu.h"
+#include "adjoint.h"
 #include "opgpu_device.h"
 #include "opgpu_host.h"
 
@@ -38,6 +39,25 @@ struct opgpu_ctx {
     int8_t *d_gstage = nullptr, *d_exist = nullptr;
     double *d_dg = nullptr, *d_pair_sigma = nullptr, *d_pair_mu = nullptr;
     double* d_dg_pair = nullptr;     // limited driving force per grain pair (G <= kMaxPairTableGrains)
+    // checkpoints of the state and the grain records (adjoint rollouts)
+    struct Slot {
+        uint8_t* cnt = nullptr; int16_t* idx = nullptr; void* val = nullptr;
+        double *volume = nullptr, *maxvol = nullptr, *vr = nullptr;
+        int8_t *exist = nullptr, *stage = nullptr;
+    };
+    std::vector<Slot> slots;
+    // adjoint / tangent-linear buffers (allocated on first use)
+    double *d_lam[2] = {nullptr, nullptr};
+    double* d_lam_local = nullptr;
+    uint8_t* d_lcnt = nullptr;
+    int16_t* d_lidx = nullptr;
+    double* d_llam = nullptr;
+    double *d_gsig = nullptr, *d_gmu = nullptr, *d_gdg = nullptr;
+    double *d_tsig = nullptr, *d_tmu = nullptr, *d_tdg = nullptr;
+    double* d_dphi[2] = {nullptr, nullptr};
+    double* d_tvol = nullptr;
+    int lam_cur = 0, dphi_cur = 0;
+    bool adjoint_ready = false, tlm_ready = false;
     bool dg_pair_dirty = true;
     uint32_t* d_status = nullptr;
     unsigned long long* d_counters = nullptr;
@@ -441,6 +461,15 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     dfree(ctx->d_bucket); dfree(ctx->d_bucket_count);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
+    for (auto& s : ctx->slots)
+    {
+        dfree(s.cnt); dfree(s.idx); dfree(s.val); dfree(s.volume); dfree(s.maxvol); dfree(s.vr);
+        dfree(s.exist); dfree(s.stage);
+    }
+    for (int b = 0; b < 2; b++) { dfree(ctx->d_lam[b]); dfree(ctx->d_dphi[b]); }
+    dfree(ctx->d_lam_local); dfree(ctx->d_lcnt); dfree(ctx->d_lidx); dfree(ctx->d_llam);
+    dfree(ctx->d_gsig); dfree(ctx->d_gmu); dfree(ctx->d_gdg);
+    dfree(ctx->d_tsig); dfree(ctx->d_tmu); dfree(ctx->d_tdg); dfree(ctx->d_tvol);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return OPGPU_OK;
@@ -954,5 +983,264 @@ extern "C" uint32_t opgpu_clear_status(opgpu_ctx* ctx)
     if (uint32_t r = require(ctx, true, "")) return r;
     read_status(ctx);
     ctx->status = 0;
+    return OPGPU_OK;
+}
+
+// ---- checkpoints, adjoint and tangent-linear model (no reference counterpart) -------------------
+namespace {
+
+StepArrays step_arrays(opgpu_ctx* ctx, const uint8_t* cnt_in, const int16_t* idx_in, const void* val_in,
+                       const double* vr, int out)
+{
+    StepArrays a{};
+    a.cnt_in = cnt_in; a.idx_in = idx_in; a.val_in = val_in;
+    a.cnt_out = ctx->cnt[out]; a.idx_out = ctx->idx[out]; a.val_out = ctx->val[out];
+    a.vr = vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
+    a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
+    a.dg_pair = (ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && !ctx->dg_pair_dirty) ? ctx->d_dg_pair : nullptr;
+    a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
+    return a;
+}
+
+uint32_t copy_state(opgpu_ctx* ctx, uint8_t* dc, int16_t* di, void* dv, const uint8_t* sc, const int16_t* si,
+                    const void* sv)
+{
+    const size_t N = (size_t)ctx->n, K = (size_t)ctx->K;
+    CK(cudaMemcpyAsync(dc, sc, N, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(di, si, N * K * sizeof(int16_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dv, sv, N * K * ctx->rsz, cudaMemcpyDeviceToDevice, ctx->stream));
+    return OPGPU_OK;
+}
+
+uint32_t copy_grains(opgpu_ctx* ctx, double* vol, double* mx, double* vr, int8_t* ex, int8_t* stg,
+                     const double* svol, const double* smx, const double* svr, const int8_t* sex, const int8_t* sstg)
+{
+    const size_t G = (size_t)ctx->G;
+    CK(cudaMemcpyAsync(vol, svol, G * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(mx, smx, G * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(vr, svr, G * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ex, sex, G, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(stg, sstg, G, cudaMemcpyDeviceToDevice, ctx->stream));
+    return OPGPU_OK;
+}
+
+// Fill the G*G driving-force table if it is out of date (the forward step does the same).
+uint32_t refresh_dg_pair(opgpu_ctx* ctx)
+{
+    if (ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && ctx->dg_pair_dirty)
+    {
+        if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, (size_t)ctx->G * ctx->G));
+        const int rc = launch_dg_pair(ctx->sp, ctx->d_dg, ctx->d_gphase, ctx->d_dg_pair, ctx->stream);
+        if (rc != 0) return fail(ctx, OPGPU_E_CUDA, "driving-force table");
+        ctx->kernel_launches++;
+        ctx->dg_pair_dirty = false;
+    }
+    return OPGPU_OK;
+}
+
+uint32_t ensure_adjoint(opgpu_ctx* ctx)
+{
+    if (ctx->adjoint_ready) return OPGPU_OK;
+    const size_t N = (size_t)ctx->n, K = (size_t)ctx->K, G = (size_t)ctx->G;
+    for (int b = 0; b < 2; b++) CK(dalloc(&ctx->d_lam[b], N * K));
+    CK(dalloc(&ctx->d_lam_local, N * K));
+    CK(dalloc(&ctx->d_lcnt, N));
+    CK(dalloc(&ctx->d_lidx, N * KAdjList));
+    CK(dalloc(&ctx->d_llam, N * KAdjList));
+    CK(dalloc(&ctx->d_gsig, G * G));
+    CK(dalloc(&ctx->d_gmu, G * G));
+    CK(dalloc(&ctx->d_gdg, G));
+    ctx->adjoint_ready = true;
+    return OPGPU_OK;
+}
+
+uint32_t ensure_tlm(opgpu_ctx* ctx)
+{
+    if (ctx->tlm_ready) return OPGPU_OK;
+    const size_t N = (size_t)ctx->n, K = (size_t)ctx->K, G = (size_t)ctx->G;
+    for (int b = 0; b < 2; b++) CK(dalloc(&ctx->d_dphi[b], N * K));
+    CK(dalloc(&ctx->d_tsig, G * G));
+    CK(dalloc(&ctx->d_tmu, G * G));
+    CK(dalloc(&ctx->d_tdg, G));
+    CK(dalloc(&ctx->d_tvol, G));
+    ctx->tlm_ready = true;
+    return OPGPU_OK;
+}
+
+// upper-triangle (a < b) copy of a symmetric G*G host table into a device table
+uint32_t upload_upper(opgpu_ctx* ctx, double* dst, const double* src)
+{
+    const size_t G = (size_t)ctx->G;
+    std::vector<double> h(G * G, 0.0);
+    if (src)
+        for (size_t a = 0; a < G; a++)
+            for (size_t b = a + 1; b < G; b++) h[a * G + b] = src[a * G + b];
+    CK(cudaMemcpyAsync(dst, h.data(), G * G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OPGPU_OK;
+}
+
+}  // namespace
+
+extern "C" uint32_t opgpu_checkpoint_reserve(opgpu_ctx* ctx, int32_t nslots)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_checkpoint_reserve: set the grains first")) return r;
+    if (nslots < 0 || nslots > 4096) return fail(ctx, OPGPU_E_INVALID, "opgpu_checkpoint_reserve: 0..4096 slots");
+    const size_t N = (size_t)ctx->n, K = (size_t)ctx->K, G = (size_t)ctx->G;
+    while ((int)ctx->slots.size() < nslots)
+    {
+        opgpu_ctx::Slot s;
+        CK(dalloc(&s.cnt, N));
+        CK(dalloc(&s.idx, N * K));
+        CK(cudaMalloc(&s.val, N * K * ctx->rsz + 16));
+        CK(dalloc(&s.volume, G)); CK(dalloc(&s.maxvol, G)); CK(dalloc(&s.vr, G));
+        CK(dalloc(&s.exist, G)); CK(dalloc(&s.stage, G));
+        ctx->slots.push_back(s);
+    }
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_checkpoint_save(opgpu_ctx* ctx, int32_t slot)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_checkpoint_save: not initialized")) return r;
+    if (slot < 0 || slot >= (int)ctx->slots.size()) return fail(ctx, OPGPU_E_INVALID, "opgpu_checkpoint_save: no such slot");
+    auto& s = ctx->slots[slot];
+    if (uint32_t r = copy_state(ctx, s.cnt, s.idx, s.val, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur])) return r;
+    return copy_grains(ctx, s.volume, s.maxvol, s.vr, s.exist, s.stage, ctx->d_volume, ctx->d_maxvol, ctx->d_vr,
+                       ctx->d_exist, ctx->d_gstage);
+}
+
+extern "C" uint32_t opgpu_checkpoint_load(opgpu_ctx* ctx, int32_t slot)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_checkpoint_load: not initialized")) return r;
+    if (slot < 0 || slot >= (int)ctx->slots.size()) return fail(ctx, OPGPU_E_INVALID, "opgpu_checkpoint_load: no such slot");
+    auto& s = ctx->slots[slot];
+    if (uint32_t r = copy_state(ctx, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur], s.cnt, s.idx, s.val)) return r;
+    if (uint32_t r = copy_grains(ctx, ctx->d_volume, ctx->d_maxvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage,
+                                 s.volume, s.maxvol, s.vr, s.exist, s.stage)) return r;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_adjoint_begin(opgpu_ctx* ctx, const double* dL_dV)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_adjoint_begin: not initialized")) return r;
+    if (!dL_dV) return fail(ctx, OPGPU_E_INVALID, "opgpu_adjoint_begin: dL_dV is NULL");
+    if (uint32_t r = ensure_adjoint(ctx)) return r;
+    const size_t G = (size_t)ctx->G;
+    double* d_w = nullptr;
+    CK(dalloc(&d_w, G));
+    CK(cudaMemcpyAsync(d_w, dL_dV, G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_lam[ctx->lam_cur], 0, (size_t)ctx->n * ctx->K * sizeof(double), ctx->stream));
+    if (launch_lambda_init(ctx->n, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], d_w, ctx->d_lam[ctx->lam_cur], ctx->stream))
+        return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_begin: launch");
+    CK(cudaMemsetAsync(ctx->d_gsig, 0, G * G * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_gmu, 0, G * G * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_gdg, 0, G * sizeof(double), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    dfree(d_w);
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->adjoint_ready, "opgpu_adjoint_step: call opgpu_adjoint_begin first")) return r;
+    if (slot < 0 || slot >= (int)ctx->slots.size()) return fail(ctx, OPGPU_E_INVALID, "opgpu_adjoint_step: no such slot");
+    if (!(dt > 0.0)) return fail(ctx, OPGPU_E_INVALID, "opgpu_adjoint_step: dt > 0 required");
+    if (uint32_t r = refresh_dg_pair(ctx)) return r;
+    auto& s = ctx->slots[slot];
+    StepParams sp = ctx->sp;
+    sp.dt = dt;
+    StepArrays a = step_arrays(ctx, s.cnt, s.idx, s.val, s.vr, 1 - ctx->cur);
+    AdjArrays aa{};
+    aa.cnt1 = ctx->cnt[ctx->cur]; aa.idx1 = ctx->idx[ctx->cur]; aa.lam1 = ctx->d_lam[ctx->lam_cur];
+    aa.lam_local = ctx->d_lam_local; aa.lcnt = ctx->d_lcnt; aa.lidx = ctx->d_lidx; aa.llam = ctx->d_llam;
+    aa.gsig = ctx->d_gsig; aa.gmu = ctx->d_gmu; aa.gdg = ctx->d_gdg;
+    double* lam0 = ctx->d_lam[1 - ctx->lam_cur];
+    CK(cudaMemsetAsync(lam0, 0, (size_t)ctx->n * ctx->K * sizeof(double), ctx->stream));
+    if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, lam0, ctx->stream))
+        return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: launch");
+    ctx->kernel_launches += 2;
+    ctx->lam_cur = 1 - ctx->lam_cur;
+    // the state before the step becomes the current state (the adjoint is aligned with it)
+    if (uint32_t r = copy_state(ctx, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur], s.cnt, s.idx, s.val)) return r;
+    if (uint32_t r = copy_grains(ctx, ctx->d_volume, ctx->d_maxvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage,
+                                 s.volume, s.maxvol, s.vr, s.exist, s.stage)) return r;
+    const uint32_t st = read_status(ctx);
+    if (st & OPGPU_E_CUDA) return st;
+    return st & OPGPU_SOFT_MASK;
+}
+
+extern "C" uint32_t opgpu_adjoint_gradients(opgpu_ctx* ctx, double* dL_dsigma, double* dL_dmu, double* dL_ddG)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->adjoint_ready, "opgpu_adjoint_gradients: no adjoint run")) return r;
+    const size_t G = (size_t)ctx->G;
+    std::vector<double> hs(G * G), hm(G * G);
+    CK(cudaMemcpyAsync(hs.data(), ctx->d_gsig, G * G * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(hm.data(), ctx->d_gmu, G * G * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (dL_ddG) CK(cudaMemcpyAsync(dL_ddG, ctx->d_gdg, G * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t a = 0; a < G; a++)
+        for (size_t b = 0; b < G; b++)
+        {
+            const size_t k = a < b ? a * G + b : b * G + a;
+            if (dL_dsigma) dL_dsigma[a * G + b] = a == b ? 0.0 : hs[k];
+            if (dL_dmu) dL_dmu[a * G + b] = a == b ? 0.0 : hm[k];
+        }
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_tlm_begin(opgpu_ctx* ctx, const double* dsigma, const double* dmu, const double* ddG)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_tlm_begin: not initialized")) return r;
+    if (ctx->fp32) return fail(ctx, OPGPU_E_INVALID, "opgpu_tlm_begin: the tangent-linear model runs the FP64 form");
+    if (uint32_t r = ensure_tlm(ctx)) return r;
+    const size_t G = (size_t)ctx->G;
+    if (uint32_t r = upload_upper(ctx, ctx->d_tsig, dsigma)) return r;
+    if (uint32_t r = upload_upper(ctx, ctx->d_tmu, dmu)) return r;
+    if (ddG) CK(cudaMemcpyAsync(ctx->d_tdg, ddG, G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    else CK(cudaMemsetAsync(ctx->d_tdg, 0, G * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_dphi[ctx->dphi_cur], 0, (size_t)ctx->n * ctx->K * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_tvol, 0, G * sizeof(double), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_tlm_step(opgpu_ctx* ctx, double dt, int32_t nsteps)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->tlm_ready, "opgpu_tlm_step: call opgpu_tlm_begin first")) return r;
+    if (nsteps < 0 || !(dt > 0.0)) return fail(ctx, OPGPU_E_INVALID, "opgpu_tlm_step: dt > 0 and nsteps >= 0 required");
+    if (uint32_t r = refresh_dg_pair(ctx)) return r;
+    StepParams sp = ctx->sp;
+    sp.dt = dt;
+    for (int s = 0; s < nsteps; s++)
+    {
+        const int in = ctx->cur, out = 1 - ctx->cur;
+        StepArrays a = step_arrays(ctx, ctx->cnt[in], ctx->idx[in], ctx->val[in], ctx->d_vr, out);
+        AdjArrays aa{};
+        aa.tsig = ctx->d_tsig; aa.tmu = ctx->d_tmu; aa.tdg = ctx->d_tdg;
+        aa.dphi_in = ctx->d_dphi[ctx->dphi_cur]; aa.dphi_out = ctx->d_dphi[1 - ctx->dphi_cur];
+        aa.tvol = ctx->d_tvol;
+        CK(cudaMemsetAsync(ctx->d_tvol, 0, (size_t)ctx->G * sizeof(double), ctx->stream));
+        CK(cudaMemsetAsync(aa.dphi_out, 0, (size_t)ctx->n * ctx->K * sizeof(double), ctx->stream));
+        if (launch_tlm_step(sp, a, aa, ctx->K, ctx->stream)) return fail(ctx, OPGPU_E_CUDA, "opgpu_tlm_step: launch");
+        grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
+            ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 1);
+        CK(cudaGetLastError());
+        ctx->kernel_launches += 2;
+        ctx->cur = out;
+        ctx->dphi_cur = 1 - ctx->dphi_cur;
+    }
+    const uint32_t st = read_status(ctx);
+    if (st & OPGPU_E_CUDA) return st;
+    return st & OPGPU_SOFT_MASK;
+}
+
+extern "C" uint32_t opgpu_tlm_volumes(opgpu_ctx* ctx, double* dV)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->tlm_ready, "opgpu_tlm_volumes: call opgpu_tlm_begin first")) return r;
+    if (!dV) return fail(ctx, OPGPU_E_INVALID, "opgpu_tlm_volumes: dV is NULL");
+    CK(cudaMemcpyAsync(dV, ctx->d_tvol, (size_t)ctx->G * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return OPGPU_OK;
 }

@@ -23,6 +23,7 @@ enum : uint32_t {
     kStNormalizeWarn = 1u << 3,
     kStLimiterCap = 1u << 4,
     kStNonFinite = 1u << 5,
+    kStAdjointMismatch = 1u << 6,   // the recomputed step does not reproduce the stored next state
 };
 
 // counters[] slots: the step kernel adds into the per-step slots 0-2; the grain-update kernel rolls

@@ -347,6 +347,100 @@ __device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& 
     return m;
 }
 
+// Periodic neighbour offsets of voxel v: X[i] + Y[j] + Z[k] is the voxel at (x+i-1, y+j-1, z+k-1).
+struct Neighbourhood {
+    long long X[3], Y[3], Z[3];
+    __device__ __forceinline__ Neighbourhood(const StepParams& p, long long v)
+    {
+        const int nx = p.nx, ny = p.ny, nz = p.nz;
+        const int z = (int)(v % nz);
+        const long long t = v / nz;
+        const int y = (int)(t % ny);
+        const int x = (int)(t / ny);
+        const long long plane = (long long)ny * nz;
+        X[0] = (long long)(x == 0 ? nx - 1 : x - 1) * plane; X[1] = (long long)x * plane;
+        X[2] = (long long)(x == nx - 1 ? 0 : x + 1) * plane;
+        Y[0] = (long long)(y == 0 ? ny - 1 : y - 1) * nz; Y[1] = (long long)y * nz;
+        Y[2] = (long long)(y == ny - 1 ? 0 : y + 1) * nz;
+        Z[0] = (z == 0 ? nz - 1 : z - 1); Z[1] = z; Z[2] = (z == nz - 1 ? 0 : z + 1);
+    }
+    __device__ __forceinline__ long long at(int dx, int dy, int dz) const { return X[dx + 1] + Y[dy + 1] + Z[dz + 1]; }
+};
+
+// Flag of voxel v from the neighbour counts (PhaseField::SetFlagsSR, src/PhaseField.cpp:953-969).
+__device__ __forceinline__ int voxel_flag(const uint8_t* cnt, const Neighbourhood& nb, long long v)
+{
+    const int c = cnt[v];
+    if (c > 1) return 2;
+    for (int q = 0; q < 27; q++)
+        if (cnt[nb.X[q / 9] + nb.Y[(q / 3) % 3] + nb.Z[q % 3]] > 1) return 1;
+    return 0;
+}
+
+// Stage 1 for one voxel from global memory: own fields (stored order), then the candidates in
+// the order CalculateDerivativesSR appends them (Laplacian stencil order and neighbour-list order,
+// then the gradient pass), each with its Laplacian summed in stencil order.  Returns the list
+// length (capacity KL; a longer list raises kStOverflowList).
+template <class R, int KL>
+__device__ __forceinline__ int gather_list(const StepParams& p, const uint8_t* __restrict__ cnt,
+                                           const int16_t* __restrict__ gin, const R* __restrict__ vin,
+                                           const Neighbourhood& nb, long long v, int16_t* gL, R* val, R* lap,
+                                           uint32_t& st)
+{
+    const long long N = p.n;
+    const int c = cnt[v];
+    int n = 0;
+    for (int s = 0; s < c; s++)
+    {
+        gL[n] = gin[s * N + v];
+        val[n] = vin[s * N + v];
+        lap[n] = R(0);
+        n++;
+    }
+    for (int q = 0; q < p.ns; q++)
+    {
+        const long long u = nb.at(p.lap_d[q][0], p.lap_d[q][1], p.lap_d[q][2]);
+        const R w = (R)p.lap_w[q];
+        const int cu = cnt[u];
+        for (int s = 0; s < cu; s++)
+        {
+            const R phi = vin[s * N + u];
+            if (phi != R(0))
+            {
+                const int g = gin[s * N + u];
+                const R l = w * phi;
+                int f = 0;
+                while (f < n && gL[f] != g) f++;
+                if (f < n) lap[f] += l;
+                else if (n < KL) { gL[n] = (int16_t)g; val[n] = R(0); lap[n] = l; n++; }
+                else st |= kStOverflowList;
+            }
+        }
+    }
+    // the gradient pass of CalculateDerivativesSR appends indices it meets first
+    for (int q = 0; q < p.ng; q++)
+    {
+        const long long u = nb.at(p.grad_d[q][0], p.grad_d[q][1], p.grad_d[q][2]);
+        const int cu = cnt[u];
+        for (int s = 0; s < cu; s++)
+        {
+            const R phi = vin[s * N + u];
+            if (phi != R(0))
+            {
+                const int g = gin[s * N + u];
+                int f = 0;
+                while (f < n && gL[f] != g) f++;
+                if (f == n)
+                {
+                    if (n < KL) { gL[n] = (int16_t)g; val[n] = R(0); lap[n] = R(0); n++; }
+                    else st |= kStOverflowList;
+                }
+            }
+        }
+    }
+    return n;
+}
+
 // One voxel of the step, reading its 3x3x3 neighbourhood straight from global memory, with its
 // working arrays in local memory (capacity KL fields).  This is the general path: the full-grid
 // kernel below and the overflow kernel of the tiled step (lists longer than the tiled kernel's
@@ -361,31 +455,11 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     const int16_t* __restrict__ gin = a.idx_in;
     const R* __restrict__ vin = static_cast<const R*>(a.val_in);
     R* __restrict__ vout = static_cast<R*>(a.val_out);
-
-    const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const int z = (int)(v % nz);
-    const long long t = v / nz;
-    const int y = (int)(t % ny);
-    const int x = (int)(t / ny);
-    const long long plane = (long long)ny * nz;
-    long long X[3], Y[3], Z[3];
-    X[0] = (long long)(x == 0 ? nx - 1 : x - 1) * plane; X[1] = (long long)x * plane;
-    X[2] = (long long)(x == nx - 1 ? 0 : x + 1) * plane;
-    Y[0] = (long long)(y == 0 ? ny - 1 : y - 1) * nz; Y[1] = (long long)y * nz;
-    Y[2] = (long long)(y == ny - 1 ? 0 : y + 1) * nz;
-    Z[0] = (z == 0 ? nz - 1 : z - 1); Z[1] = z; Z[2] = (z == nz - 1 ? 0 : z + 1);
+    const Neighbourhood nb(p, v);
 
     const int c = cnt[v];
     if (count_in) ein = c;
-    int flag = c > 1 ? 2 : 0;
-    if (flag == 0)
-    {
-        for (int q = 0; q < 27 && flag == 0; q++)
-        {
-            const long long u = X[q / 9] + Y[(q / 3) % 3] + Z[q % 3];
-            if (cnt[u] > 1) flag = 1;
-        }
-    }
+    const int flag = voxel_flag(cnt, nb, v);
 
     if (flag == 0)
     {
@@ -408,55 +482,7 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     int16_t gL[KL];
     R val[KL], lap[KL], sg[KP];
     double pv[KP], pos[KL], neg[KL];
-    int n = 0;
-    for (int s = 0; s < c; s++)
-    {
-        gL[n] = gin[s * N + v];
-        val[n] = vin[s * N + v];
-        lap[n] = R(0);
-        n++;
-    }
-    for (int q = 0; q < p.ns; q++)
-    {
-        const long long u = X[p.lap_d[q][0] + 1] + Y[p.lap_d[q][1] + 1] + Z[p.lap_d[q][2] + 1];
-        const R w = (R)p.lap_w[q];
-        const int cu = cnt[u];
-        for (int s = 0; s < cu; s++)
-        {
-            const R phi = vin[s * N + u];
-            if (phi != R(0))
-            {
-                const int g = gin[s * N + u];
-                const R l = w * phi;
-                int f = 0;
-                while (f < n && gL[f] != g) f++;
-                if (f < n) lap[f] += l;
-                else if (n < KL) { gL[n] = (int16_t)g; val[n] = R(0); lap[n] = l; n++; }
-                else st |= kStOverflowList;
-            }
-        }
-    }
-    // the gradient pass of CalculateDerivativesSR appends indices it meets first
-    for (int q = 0; q < p.ng; q++)
-    {
-        const long long u = X[p.grad_d[q][0] + 1] + Y[p.grad_d[q][1] + 1] + Z[p.grad_d[q][2] + 1];
-        const int cu = cnt[u];
-        for (int s = 0; s < cu; s++)
-        {
-            const R phi = vin[s * N + u];
-            if (phi != R(0))
-            {
-                const int g = gin[s * N + u];
-                int f = 0;
-                while (f < n && gL[f] != g) f++;
-                if (f == n)
-                {
-                    if (n < KL) { gL[n] = (int16_t)g; val[n] = R(0); lap[n] = R(0); n++; }
-                    else st |= kStOverflowList;
-                }
-            }
-        }
-    }
+    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, st);
     const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1};
     int m = list_step<R>(p, a, sc, n, flag, st);
     if (m > KS) { st |= kStOverflowK; m = KS; }
