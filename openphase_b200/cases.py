@@ -44,12 +44,57 @@ class Case:
     regularization: float = 1.0
     tj_factor: float = 0.0
     name: str = ""
+    # multi-phase set-ups (default: one solid phase holding every grain, ISO energy sigma, mu)
+    phase_sigma: Optional[tuple] = None        # P x P interface energy per phase pair
+    phase_mu: Optional[tuple] = None           # P x P mobility per phase pair
+    phase_solid: Optional[tuple] = None        # per phase: 1 solid, 0 liquid
+    phase_cubic_eps: Optional[tuple] = None    # P x P: CUBIC energy model with this epsilon (0 = ISO)
+    phase_dg: Optional[tuple] = None           # per-phase driving force: dG(g) = phase_dg[phase(g)]
+    init: str = "voronoi"                      # "voronoi" or "nuclei" (grain 0 = matrix)
+    nucleus_radius: float = 4.0
+    orientations: bool = False                 # random unit quaternion per grain
 
     @property
     def n(self) -> int:
         return self.nx * self.ny * self.nz
 
+    @property
+    def nphases(self) -> int:
+        return len(self.phase_sigma) if self.phase_sigma else 1
+
+    def sigma_phase(self) -> np.ndarray:
+        return np.array(self.phase_sigma, dtype=np.float64) if self.phase_sigma else np.array([[self.sigma]])
+
+    def mu_phase(self) -> np.ndarray:
+        return np.array(self.phase_mu, dtype=np.float64) if self.phase_mu else np.array([[self.mu]])
+
+    def limit_phase(self) -> np.ndarray:
+        return np.full((self.nphases, self.nphases), self.limit)
+
+    def solid_phase(self) -> np.ndarray:
+        return np.array(self.phase_solid if self.phase_solid else (1,) * self.nphases, dtype=np.int32)
+
+    def cubic_eps(self) -> Optional[np.ndarray]:
+        return np.array(self.phase_cubic_eps, dtype=np.float64) if self.phase_cubic_eps else None
+
+    def energy_models(self) -> Optional[np.ndarray]:
+        """P x P model codes: 0 ISO, 1 CUBIC."""
+        e = self.cubic_eps()
+        return None if e is None else (e != 0.0).astype(np.int32)
+
+    def grain_phase(self) -> np.ndarray:
+        g = np.zeros(self.ngrains, dtype=np.int32)
+        if self.init == "nuclei":
+            g[1:] = 1
+        return g
+
+    def quaternions(self) -> Optional[np.ndarray]:
+        return init.quaternions(self.ngrains, self.seed) if self.orientations else None
+
     def initial_state(self, threads: int = 0):
+        if self.init == "nuclei":
+            return init.nuclei(self.nx, self.ny, self.nz, self.ngrains, self.seed, self.nucleus_radius,
+                               self.iwidth)
         return init.voronoi(self.nx, self.ny, self.nz, self.ngrains, self.seed, threads)
 
     def pair_sigma(self) -> Optional[np.ndarray]:
@@ -59,6 +104,8 @@ class Case:
         return init.sigma_table(self.ngrains, self.seed, lo, span)
 
     def driving_force(self) -> Optional[np.ndarray]:
+        if self.phase_dg:
+            return np.array(self.phase_dg, dtype=np.float64)[self.grain_phase()]
         if not self.dg_scale:
             return None
         return init.driving_forces(self.ngrains, self.seed, self.dg_scale)
@@ -83,6 +130,16 @@ def grain_growth_dg_128() -> Case:
     kernel profiles are captured on."""
     return Case(128, 128, 128, 250, seed=2, iwidth=6.0, dt=0.08, nsteps=2000, sigma=1.2, mu=1.0,
                 sigma_pairs=(0.8, 0.4), dg_scale=0.05, name="grain_growth_dg_128")
+
+
+def solidification_128() -> Case:
+    """Liquid (grain 0, phase 0) with 64 solid nuclei of radius 4 (phase 1), liquid -> solid driving
+    force 0.1, solid-liquid sigma = 1.0 with cubic anisotropy eps = 0.02 and per-nucleus random
+    orientations, solid-solid sigma = 1.2, mu_sl = 2.0, mu_ss = 0.5, eta = 5 dx, dt = 0.05."""
+    return Case(128, 128, 128, 65, seed=3, iwidth=5.0, dt=0.05, nsteps=1500, sigma=1.2,
+                phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)), phase_solid=(0, 1),
+                phase_cubic_eps=((0.0, 0.02), (0.02, 0.0)), phase_dg=(0.1, 0.0), init="nuclei",
+                nucleus_radius=4.0, orientations=True, name="solidification_128")
 
 
 def adjoint_calibration_128() -> Case:

@@ -412,6 +412,29 @@ __device__ __forceinline__ bool limiter_iteration(int n, const double* val, doub
     return needed;
 }
 
+// Sums and limits of one limiter iteration for the increments pv (pv itself is not changed).
+__device__ __forceinline__ void limiter_limits(int n, const double* val, double dt, const double* pv, double* pos,
+                                               double* neg, double* limN, double* limP)
+{
+    for (int i = 0; i < n; i++) { pos[i] = 0.0; neg[i] = 0.0; }
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++)
+        {
+            const double w = pv[pair_pos(i, j, n)];
+            if (w < 0.0) { neg[i] += w; pos[j] += -w; }
+            if (w > 0.0) { pos[i] += w; neg[j] += -w; }
+        }
+    for (int i = 0; i < n; i++)
+    {
+        const double vi = val[i], pi = pos[i], ni = neg[i];
+        const double newPF = vi + (pi + ni) * dt;
+        limN[i] = 1.0;
+        limP[i] = 1.0;
+        if (newPF < 0.0) limN[i] = dmin_ref(1.0, -(vi + pi * dt) / (ni * dt));
+        if (newPF > 1.0) limP[i] = dmin_ref(1.0, (1.0 - (vi + ni * dt)) / (pi * dt));
+    }
+}
+
 // Reverse of one limiter iteration: pv_in is the input of the iteration (restored), lout the adjoint
 // of its output; returns the adjoint of its input in lin and adds to lval.
 __device__ void limiter_iteration_reverse(int n, const double* val, double dt, const double* pv_in,
@@ -419,10 +442,7 @@ __device__ void limiter_iteration_reverse(int n, const double* val, double dt, c
                                           double* limN, double* limP, double* lpos, double* lneg)
 {
     // forward quantities of this iteration
-    double tmp[KAdjPairs];
-    const int np = n * (n - 1) / 2;
-    for (int q = 0; q < np; q++) tmp[q] = pv_in[q];
-    limiter_iteration(n, val, dt, tmp, pos, neg, limN, limP);
+    limiter_limits(n, val, dt, pv_in, pos, neg, limN, limP);
     double llimN[KAdjList], llimP[KAdjList];
     for (int i = 0; i < n; i++) { llimN[i] = 0.0; llimP[i] = 0.0; lpos[i] = 0.0; lneg[i] = 0.0; }
     for (int i = 0; i < n; i++)
@@ -726,7 +746,7 @@ __global__ void __launch_bounds__(64) adjoint_local_kernel(const __grid_constant
             if (dropped) lpv[q] = 0.0;
         }
         // limiter iterations in reverse; the input of iteration r is rebuilt from the zeroed increments
-        double pin[KP];
+        double* pin = pv;   // the forward's increments are no longer needed
         for (int r = iters; r >= 1; r--)
         {
             for (int q = 0; q < np; q++) pin[q] = pv0[q];

@@ -1156,8 +1156,7 @@ extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
     aa.cnt1 = ctx->cnt[ctx->cur]; aa.idx1 = ctx->idx[ctx->cur]; aa.lam1 = ctx->d_lam[ctx->lam_cur];
     aa.lam_local = ctx->d_lam_local; aa.lcnt = ctx->d_lcnt; aa.lidx = ctx->d_lidx; aa.llam = ctx->d_llam;
     aa.gsig = ctx->d_gsig; aa.gmu = ctx->d_gmu; aa.gdg = ctx->d_gdg;
-    double* lam0 = ctx->d_lam[1 - ctx->lam_cur];
-    CK(cudaMemsetAsync(lam0, 0, (size_t)ctx->n * ctx->K * sizeof(double), ctx->stream));
+    double* lam0 = ctx->d_lam[1 - ctx->lam_cur];   // every stored entry of the slot's state is written
     if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, lam0, ctx->stream))
         return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: launch");
     ctx->kernel_launches += 2;

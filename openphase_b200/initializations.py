@@ -110,3 +110,72 @@ def parse_raw(data: bytes):
     idx = words[entry_pos].astype(np.int32)
     val = words[entry_pos + 1].view(np.float64).copy()
     return (int(nx), int(ny), int(nz)), counts, idx, val
+
+
+STREAM_ORIENTATION = 5
+
+
+def nucleus_centres(ngrains: int, nx: int, ny: int, nz: int, seed: int) -> np.ndarray:
+    """Centres of nuclei 1..ngrains-1 (grain 0 is the matrix): u(seed, POSITION, g, axis)*n."""
+    c = np.empty((ngrains, 3))
+    for g in range(ngrains):
+        for ax, n in enumerate((nx, ny, nz)):
+            c[g, ax] = uniform(seed, STREAM_POSITION, g, ax) * n
+    return c
+
+
+def nuclei(nx: int, ny: int, nz: int, ngrains: int, seed: int, radius: float, iwidth: float):
+    """Grain 0 fills the box; grains 1..ngrains-1 are spheres of the given radius at seeded centres
+    with the diffuse profile of Initializations::Sphere (src/Initializations.cpp:341-389): inside
+    R - iWidth/2 the voxel holds only the sphere; out to R + iWidth/2 the sphere gets
+    p = 0.5 - 0.5*sin(pi*(r - R)/iWidth) and the values already present are scaled by 1 - p.
+    Distances are periodic minimum-image distances to the centre; nuclei are placed in index order.
+    Returns ragged lists (counts, idx, val) (not normalised; finalize normalises)."""
+    N = nx * ny * nz
+    lists = [dict() for _ in range(N)]
+    for v in range(N):
+        lists[v][0] = 1.0
+    centres = nucleus_centres(ngrains, nx, ny, nz, seed)
+    reach = int(np.ceil(radius + 0.5 * iwidth)) + 1
+    for g in range(1, ngrains):
+        cx, cy, cz = centres[g]
+        ix = np.arange(int(np.floor(cx)) - reach, int(np.floor(cx)) + reach + 2)
+        iy = np.arange(int(np.floor(cy)) - reach, int(np.floor(cy)) + reach + 2)
+        iz = np.arange(int(np.floor(cz)) - reach, int(np.floor(cz)) + reach + 2)
+        seen = set()
+        for i in ix:
+            for j in iy:
+                for k in iz:
+                    v = ((i % nx) * ny + (j % ny)) * nz + (k % nz)
+                    if v in seen:
+                        continue
+                    seen.add(v)
+                    dx = min(abs(i % nx - cx), nx - abs(i % nx - cx))
+                    dy = min(abs(j % ny - cy), ny - abs(j % ny - cy))
+                    dz = min(abs(k % nz - cz), nz - abs(k % nz - cz))
+                    rad = float(np.sqrt(dx * dx + dy * dy + dz * dz))
+                    if rad < radius - 0.5 * iwidth:
+                        lists[v] = {g: 1.0}
+                    elif rad <= radius + 0.5 * iwidth:
+                        prof = 0.5 - 0.5 * np.sin(np.pi * (rad - radius) / iwidth)
+                        for key in lists[v]:
+                            lists[v][key] *= 1.0 - prof
+                        lists[v][g] = prof
+    counts = np.array([len(d) for d in lists], dtype=np.int32)
+    idx = np.fromiter((k for d in lists for k in d), dtype=np.int32, count=int(counts.sum()))
+    val = np.fromiter((x for d in lists for x in d.values()), dtype=np.float64, count=int(counts.sum()))
+    return counts, idx, val
+
+
+def quaternions(ngrains: int, seed: int) -> np.ndarray:
+    """Uniform random unit quaternions (s, x, y, z) per grain by Shoemake's method (Graphics Gems
+    III, 1992): u1, u2, u3 uniform; q = (sqrt(1-u1) sin 2pi u2, sqrt(1-u1) cos 2pi u2,
+    sqrt(u1) sin 2pi u3, sqrt(u1) cos 2pi u3)."""
+    q = np.empty((ngrains, 4))
+    for g in range(ngrains):
+        u1, u2, u3 = (uniform(seed, STREAM_ORIENTATION, g, k) for k in range(3))
+        a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+        x, y = a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2)
+        z, w = b * np.sin(2 * np.pi * u3), b * np.cos(2 * np.pi * u3)
+        q[g] = (w, x, y, z)
+    return q

@@ -91,18 +91,29 @@ class Oracle:
             return a
 
         G = case.ngrains
-        sig = keep(np.array([[case.sigma]], dtype=np.float64))
-        mu = keep(np.array([[case.mu]], dtype=np.float64))
-        lim = keep(np.array([[case.limit]], dtype=np.float64))
+        P = case.nphases
+        sig = keep(case.sigma_phase())
+        mu = keep(case.mu_phase())
+        lim = keep(case.limit_phase())
+        gph = keep(case.grain_phase().astype(np.int32))
+        sol = keep(case.solid_phase().astype(np.int32))
+        em = case.energy_models()
+        em = keep(em.astype(np.int32)) if em is not None else None
+        eps = case.cubic_eps()
+        eps = keep(eps) if eps is not None else None
+        quat = case.quaternions()
+        quat = keep(quat.astype(np.float64)) if quat is not None else None
         ps = case.pair_sigma()
         ps = keep(ps.astype(np.float64)) if ps is not None else None
         dg = case.driving_force()
         dg = keep(dg) if dg is not None else None
         p = OpParams(nx=case.nx, ny=case.ny, nz=case.nz, dx=case.dx, iwidth=case.iwidth,
                      stencil=STENCIL[case.stencil], gradient_stencil=STENCIL[case.gradient_stencil],
-                     nphases=1, ngrains=G, grain_phase=None, phase_solid=None,
-                     sigma_phase=_p(sig).value, mu_phase=_p(mu).value, energy_model=None, cubic_eps=None,
-                     quat=None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
+                     nphases=P, ngrains=G, grain_phase=_p(gph).value, phase_solid=_p(sol).value,
+                     sigma_phase=_p(sig).value, mu_phase=_p(mu).value,
+                     energy_model=_p(em).value if em is not None else None,
+                     cubic_eps=_p(eps).value if eps is not None else None,
+                     quat=_p(quat).value if quat is not None else None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
                      dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
                      limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
                      consider_nucleus_volume=1, nucleus_volume_factor=1.0, threads=threads)
@@ -169,12 +180,30 @@ def reference_available() -> bool:
 
 
 def _case_text(case, workdir: Path, dump_steps, threads):
+    P = case.nphases
     lines = [f"nx {case.nx}", f"ny {case.ny}", f"nz {case.nz}", f"dx {case.dx!r}", f"iwidth {case.iwidth!r}",
-             f"stencil {case.stencil}", f"dt {case.dt!r}", f"nsteps {max(dump_steps)}", "nphases 1",
-             f"sigma 0 0 {case.sigma!r}", f"mu 0 0 {case.mu!r}", f"limit 0 0 {case.limit!r}",
+             f"stencil {case.stencil}", f"dt {case.dt!r}", f"nsteps {max(dump_steps)}", f"nphases {P}",
              f"ngrains {case.ngrains}", f"limiting {int(case.limiting)}",
              f"regularization {case.regularization!r}", f"tj_factor {case.tj_factor!r}",
              "dump_steps " + " ".join(str(s) for s in dump_steps)]
+    sig, mu, lim, sol = case.sigma_phase(), case.mu_phase(), case.limit_phase(), case.solid_phase()
+    eps = case.cubic_eps()
+    for a in range(P):
+        lines.append(f"phase_state {a} {'SOLID' if sol[a] else 'LIQUID'}")
+        for b in range(a, P):
+            lines += [f"sigma {a} {b} {float(sig[a, b])!r}", f"mu {a} {b} {float(mu[a, b])!r}",
+                      f"limit {a} {b} {float(lim[a, b])!r}"]
+            if eps is not None and eps[a, b] != 0.0:
+                lines += [f"energy_model {a} {b} CUBIC", f"cubic_eps {a} {b} {float(eps[a, b])!r}"]
+    if P > 1:
+        f = workdir / "grain_phase.bin"
+        case.grain_phase().astype(np.int32).tofile(f)
+        lines.append(f"grain_phase_file {f}")
+    quat = case.quaternions()
+    if quat is not None:
+        f = workdir / "orientation.bin"
+        np.ascontiguousarray(quat, dtype=np.float64).tofile(f)
+        lines.append(f"orientation_file {f}")
     if threads:
         lines.append(f"threads {threads}")
     ps = case.pair_sigma()

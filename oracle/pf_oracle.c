@@ -32,6 +32,10 @@ struct op_sim {
     int* grain_phase;
     int* phase_solid;
     double *sigma_phase, *mu_phase, *limit_phase, *pair_sigma, *pair_mu, *dg;
+    int* energy_model;            /* [P*P] OP_ENERGY_*                                           */
+    double* cubic_eps;            /* [P*P]                                                       */
+    double* rot;                  /* [G*9] grain RotationMatrix, row-major                       */
+    int aniso;                    /* some phase pair uses an anisotropic energy model            */
     long n;
     int cap;
     int32_t* cnt;   entry* e;     /* Fields                                */
@@ -137,7 +141,44 @@ op_sim* op_create(const op_params* p, int cap)
     s->p.grain_phase = s->grain_phase; s->p.phase_solid = s->phase_solid;
     s->p.sigma_phase = s->sigma_phase; s->p.mu_phase = s->mu_phase; s->p.limit_phase = s->limit_phase;
     s->p.pair_sigma = s->pair_sigma; s->p.pair_mu = s->pair_mu; s->p.dg = s->dg;
-    s->p.energy_model = NULL; s->p.cubic_eps = NULL; s->p.quat = NULL;
+    s->energy_model = (int*)calloc((size_t)P*P, sizeof(int));
+    s->cubic_eps = (double*)calloc((size_t)P*P, sizeof(double));
+    s->aniso = 0;
+    for (int q = 0; q < P*P; q++)
+    {
+        if (p->energy_model) s->energy_model[q] = p->energy_model[q];
+        if (p->cubic_eps) s->cubic_eps[q] = p->cubic_eps[q];
+        if (s->energy_model[q] != OP_ENERGY_ISO) s->aniso = 1;
+    }
+    /* Quaternion::setRotationMatrix (src/Containers/Quaternion.cpp:78-98) of each grain's
+     * orientation, normalised as Quaternion::normalized (include/Containers/Quaternion.h:304-311);
+     * unit rotation without orientations. */
+    s->rot = (double*)calloc((size_t)G*9, sizeof(double));
+    for (int g = 0; g < G; g++)
+    {
+        double* R = s->rot + 9*g;
+        const double qs = p->quat ? p->quat[4*g] : 1.0;
+        const double q0 = p->quat ? p->quat[4*g + 1] : 0.0;
+        const double q1 = p->quat ? p->quat[4*g + 2] : 0.0;
+        const double q2 = p->quat ? p->quat[4*g + 3] : 0.0;
+        const double len = sqrt(qs*qs + q0*q0 + q1*q1 + q2*q2);
+        if (len < DBL_EPSILON)
+        {
+            R[0] = 1.0; R[4] = 1.0; R[8] = 1.0;
+            continue;
+        }
+        const double S = qs/len, V0 = q0/len, V1 = q1/len, V2 = q2/len;
+        R[0] = 1.0 - 2.0*(V1*V1 + V2*V2);
+        R[1] =       2.0*(V0*V1 -  S*V2);
+        R[2] =       2.0*(V0*V2 +  S*V1);
+        R[3] =       2.0*(V0*V1 +  S*V2);
+        R[4] = 1.0 - 2.0*(V0*V0 + V2*V2);
+        R[5] =       2.0*(V1*V2 -  S*V0);
+        R[6] =       2.0*(V0*V2 -  S*V1);
+        R[7] =       2.0*(V1*V2 +  S*V0);
+        R[8] = 1.0 - 2.0*(V0*V0 + V1*V1);
+    }
+    s->p.energy_model = s->energy_model; s->p.cubic_eps = s->cubic_eps; s->p.quat = NULL;
     if (s->p.nucleus_volume_factor == 0.0) s->p.nucleus_volume_factor = 1.0;
     s->n = (long)p->nx * p->ny * p->nz;
     s->cap = cap;
@@ -173,6 +214,7 @@ void op_destroy(op_sim* s)
     free(s->grain_phase); free(s->phase_solid);
     free(s->sigma_phase); free(s->mu_phase); free(s->limit_phase);
     free(s->pair_sigma); free(s->pair_mu); free(s->dg);
+    free(s->energy_model); free(s->cubic_eps); free(s->rot);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
     free(s->exist); free(s->stage);
@@ -232,6 +274,84 @@ static double phase_energy(const op_sim* s, int pa, int pb)
     return s->sigma_phase[pa*s->p.nphases + pb];
 }
 
+/* InterfaceEnergyModel::MaxEnergy of a phase pair: Energy for ISO (ReadInputIso), Energy*(1 +
+ * Epsilon1*1.41) for CUBIC (ReadInputCubic, include/InterfaceProperties/InterfaceEnergyModel.h:78-94). */
+static double phase_max_energy(const op_sim* s, int pa, int pb)
+{
+    const int q = pa*s->p.nphases + pb;
+    if (s->energy_model[q] == OP_ENERGY_CUBIC) return s->sigma_phase[q]*(1.0 + s->cubic_eps[q]*1.41);
+    return s->sigma_phase[q];
+}
+
+/* InterfaceOrientation (src/InterfaceProperties.cpp:39-45): the normal -grad(phi) normalised
+ * (dVector3::normalize, include/Containers/dVector3.h:301-316) and rotated back to the grain's
+ * reference frame with the transposed RotationMatrix (MatrixVectorOperators.h:43-52). */
+static void interface_orientation(const op_sim* s, const entry* e, double out[3])
+{
+    double n[3] = {e->grad[0]*(-1.0), e->grad[1]*(-1.0), e->grad[2]*(-1.0)};
+    const double norm = sqrt(n[0]*n[0] + n[1]*n[1] + n[2]*n[2]);
+    if (norm > DBL_EPSILON)
+    {
+        const double inv = 1.0/norm;
+        n[0] *= inv; n[1] *= inv; n[2] *= inv;
+    }
+    else
+    {
+        n[0] = 0.0; n[1] = 0.0; n[2] = 0.0;
+    }
+    const double* R = s->rot + 9*e->idx;
+    for (int i = 0; i < 3; i++)
+    {
+        double t = 0.0;
+        for (int j = 0; j < 3; j++) t += R[3*j + i]*n[j];
+        out[i] = t;
+    }
+}
+
+/* InterfaceEnergyModel::Calculate, CUBIC (InterfaceEnergyModel.h:325-345). */
+static double cubic_energy(double energy, double eps, const double n[3])
+{
+    return energy*(1.0 + eps*(1.5 - 2.5*(pow(n[0], 4) + pow(n[1], 4) + pow(n[2], 4))));
+}
+
+/* The energy InterfaceProperties::SetSR (src/InterfaceProperties.cpp:617-673) stores for the pair of
+ * list entries a, b of one voxel: ISO (or the per-grain-pair table) as ip_energy; an anisotropic
+ * model averages the model energy of each solid grain's interface orientation, weighted by
+ * |phi(1 - phi)|, falling back to MaxEnergy when neither weight exceeds DBL_EPSILON. */
+static double voxel_energy(const op_sim* s, const entry* L, int a, int b)
+{
+    const int ga = L[a].idx, gb = L[b].idx;
+    const int pA = s->grain_phase[ga], pB = s->grain_phase[gb];
+    const int q = pA*s->p.nphases + pB;
+    if (s->energy_model[q] == OP_ENERGY_ISO) return ip_energy(s, ga, gb);
+    double loc = 0.0, wA = 0.0, wB = 0.0;
+    if (s->phase_solid[pA])
+    {
+        wA = fabs(L[a].val*(1.0 - L[a].val));
+        if (wA > DBL_EPSILON)
+        {
+            double n[3];
+            interface_orientation(s, &L[a], n);
+            loc += cubic_energy(s->sigma_phase[q], s->cubic_eps[q], n)*wA;
+        }
+        else wA = 0.0;
+    }
+    if (s->phase_solid[pB])
+    {
+        wB = fabs(L[b].val*(1.0 - L[b].val));
+        if (wB > DBL_EPSILON)
+        {
+            double n[3];
+            interface_orientation(s, &L[b], n);
+            loc += cubic_energy(s->sigma_phase[q], s->cubic_eps[q], n)*wB;
+        }
+        else wB = 0.0;
+    }
+    if (wA + wB > DBL_EPSILON) loc /= wA + wB;
+    else loc = phase_max_energy(s, pA, pB);
+    return loc;
+}
+
 /* PhaseField::LocalN (include/PhaseField.h:84-95) */
 static double local_n(const op_sim* s, const entry* L, int n)
 {
@@ -267,7 +387,7 @@ static int do_increments(const op_sim* s, const entry* L, int n, pair* P)
     {
         const int ga = L[a].idx, gb = L[b].idx;
         const double scale = sqrt(s->vr[ga]*s->vr[gb]);
-        double dPhi_dt = ip_energy(s, ga, gb)
+        double dPhi_dt = (s->aniso ? voxel_energy(s, L, a, b) : ip_energy(s, ga, gb))
                          *((L[a].lap + 0.5*(1.0 + scale)*Prefactor*L[a].val) -
                            (L[b].lap + 0.5*(1.0 + scale)*Prefactor*L[b].val));
         if (n > 2)
@@ -275,7 +395,8 @@ static int do_increments(const op_sim* s, const entry* L, int n, pair* P)
         if (c != a && c != b)
         {
             const int gc = L[c].idx;
-            dPhi_dt += (ip_energy(s, gb, gc) - ip_energy(s, ga, gc))
+            dPhi_dt += (s->aniso ? voxel_energy(s, L, b, c) - voxel_energy(s, L, a, c)
+                                 : ip_energy(s, gb, gc) - ip_energy(s, ga, gc))
                       *(L[c].lap + 0.5*(1.0 + scale)*Prefactor*L[c].val);
             /* TripleJunctionModels::Model (:536-552) */
             if (s->p.tj_factor != 0.0 || scale < 1.0)
@@ -313,7 +434,7 @@ static void df_merge(const op_sim* s, const entry* L, int n, pair* P)
         {
             const int pA = s->grain_phase[ga], pB = s->grain_phase[gb];
             const double lim = s->limit_phase ? s->limit_phase[pA*NP + pB] : 0.95;
-            double allowedDG = lim*Prefactor*phase_energy(s, pA, pB);   /* ISO: MaxEnergy = Energy */
+            double allowedDG = lim*Prefactor*phase_max_energy(s, pA, pB);
             allowedDG *= s->p.regularization;
             locdG = allowedDG*tanh(locdG/allowedDG);
         }

@@ -55,6 +55,7 @@ struct Case
     int nsteps = 0;
     int nphases = 1;
     std::vector<std::string> phase_state;
+    std::vector<double> quat;      // [G*4] grain orientations (s, x, y, z), empty: none
     std::map<std::pair<int,int>, double> sigma, mu, limit, cubic_eps;
     std::map<std::pair<int,int>, std::string> energy_model;
     int ngrains = 0;
@@ -96,7 +97,7 @@ static Case parse_case(const std::string& path)
     std::ifstream f(path);
     if (!f) { fprintf(stderr, "ref_driver: cannot open %s\n", path.c_str()); exit(2); }
     std::string line;
-    std::string grain_phase_file, pair_sigma_file, pair_mu_file, dg_file;
+    std::string grain_phase_file, pair_sigma_file, pair_mu_file, dg_file, orientation_file;
     while (std::getline(f, line))
     {
         std::istringstream is(line);
@@ -122,6 +123,7 @@ static Case parse_case(const std::string& path)
         else if (key == "pair_sigma_file") is >> pair_sigma_file;
         else if (key == "pair_mu_file") is >> pair_mu_file;
         else if (key == "dg_file") is >> dg_file;
+        else if (key == "orientation_file") is >> orientation_file;
         else if (key == "limiting") { int v; is >> v; c.limiting = v != 0; }
         else if (key == "regularization") is >> c.regularization;
         else if (key == "tj_factor") is >> c.tj_factor;
@@ -133,6 +135,7 @@ static Case parse_case(const std::string& path)
     if (c.phase_state.empty()) c.phase_state.assign(c.nphases, "SOLID");
     const size_t G = c.ngrains;
     c.grain_phase = grain_phase_file.empty() ? std::vector<int>(G, 0) : read_ints(grain_phase_file, G);
+    if (!orientation_file.empty()) c.quat = read_doubles(orientation_file, 4*G);
     if (!pair_sigma_file.empty()) c.pair_sigma = read_doubles(pair_sigma_file, G*G);
     if (!pair_mu_file.empty())    c.pair_mu    = read_doubles(pair_mu_file, G*G);
     if (!dg_file.empty())         c.dg         = read_doubles(dg_file, G);
@@ -171,7 +174,7 @@ static void write_opi(const Case& c, const std::string& path)
         if (model == "CUBIC")
         {
             double e = c.cubic_eps.count({a,b}) ? c.cubic_eps.at({a,b}) : 0.0;
-            o << "$Eps_" << a << "_" << b << " : " << e << "\n";
+            o << "$EpsilonE_" << a << "_" << b << " : " << e << "\n";
         }
         o << "$MobilityModel_" << a << "_" << b << " : ISO\n";
         o << "$Mu_" << a << "_" << b << " : " << m << "\n";
@@ -237,6 +240,14 @@ int main(int argc, char* argv[])
     BoundaryConditions  BC(S, opi);
 
     for (int g = 0; g < c.ngrains; g++) Phi.AddGrainInfo(c.grain_phase[g]);
+    if (!c.quat.empty())
+    {
+        // grain orientations (s, x, y, z) per grain: GrainsProperties::Orientation
+        // (include/GrainsProperties.h:76) with its rotation matrix
+        const std::vector<double>& q = c.quat;
+        for (int g = 0; g < c.ngrains; g++)
+            Phi.FieldsProperties[g].Orientation = Quaternion({q[4*g], q[4*g + 1], q[4*g + 2], q[4*g + 3]});
+    }
     if (!Phi.Read(raw_in)) { fprintf(stderr, "ref_driver: Read failed\n"); return 3; }
     Phi.FinalizeInitialization(BC);
     if (c.dump_steps.count(0)) dump(c, Phi, out, 0);

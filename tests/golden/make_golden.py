@@ -5,7 +5,7 @@ API by oracle/ref_driver.cpp) on small seeded cases and stores, per case, the st
 records at a few checkpoints.  The fixtures pin the oracle (tests/test_oracle.py) without needing the
 reference at test time.
 
-    python tests/golden/make_golden.py            # writes tests/golden/*.npz
+    python tests/golden/make_golden.py [name ...]  # writes tests/golden/<name>.npz (all by default)
 """
 from __future__ import annotations
 
@@ -30,11 +30,20 @@ GOLDEN_CASES = {
                          dg_scale=0.05, name="pairs_dg_24"), [1, 60]),
     "dg_strong_20": (Case(20, 20, 20, 40, seed=9, iwidth=4.0, dt=0.1, sigma=1.2, sigma_pairs=(0.8, 0.4),
                           dg_scale=0.3, name="dg_strong_20"), [1, 60]),
+    # liquid + solid nuclei (VolumeRatio < 1, triple-junction term), CUBIC solid-liquid energy with
+    # per-grain orientations (gradients of the candidate lists), liquid -> solid driving force
+    "cubic_nuclei_24": (Case(24, 24, 24, 7, seed=3, iwidth=5.0, dt=0.05, sigma=1.2,
+                             phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                             phase_solid=(0, 1), phase_cubic_eps=((0.0, 0.02), (0.02, 0.0)), phase_dg=(0.1, 0.0),
+                             init="nuclei", nucleus_radius=4.0, orientations=True, name="cubic_nuclei_24"),
+                        [1, 10, 40]),
 }
 
 
-def main():
+def main(names=None):
     for name, (case, steps) in GOLDEN_CASES.items():
+        if names and name not in names:
+            continue
         counts, idx, val = case.initial_state()
         res, stats = run_reference(case, counts, idx, val, [0] + steps, threads=4)
         arrays = {"init_counts": counts.astype(np.uint8), "init_idx": idx.astype(np.int16)}
@@ -52,4 +61,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
