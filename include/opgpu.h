@@ -77,6 +77,12 @@ typedef struct opgpu_model {
     double  tj_factor;             /* $TripleJunctionFactor (default 0.0)                         */
     int32_t consider_nucleus_volume; /* default 1                                                 */
     double  nucleus_volume_factor;   /* default 1.0                                               */
+    /* Anisotropic interface energy (InterfaceEnergyModel.h:78-94, 325-345; InterfaceProperties.cpp:
+     * 617-673); any may be NULL (all ISO, all phases solid). */
+    const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC ($EnergyModel_a_b)                 */
+    const double* cubic_eps;       /* [P*P] CUBIC strength ($EpsilonE_a_b)                        */
+    const int32_t* phase_solid;    /* [P] 1 = Solid, 0 = Liquid ($State_p); anisotropy weights
+                                      only count solid grains                                     */
 } opgpu_model;
 
 typedef struct opgpu_stats {
@@ -125,6 +131,9 @@ uint32_t opgpu_set_pair_hash(opgpu_ctx* ctx, uint64_t seed, double lo, double sp
  * src/DrivingForce.cpp:176-183, NodeDF.h:412-435, then Average->SkipAverage :242-274).
  * NULL disables the driving-force merge. */
 uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG);
+/* Grain orientations as quaternions (s, x, y, z) per grain, quat[4*G] (GrainsProperties::Orientation,
+ * include/GrainsProperties.h:76); NULL = unrotated.  Used by anisotropic energy models. */
+uint32_t opgpu_set_orientations(opgpu_ctx* ctx, const double* quat);
 
 /* ---- state ---------------------------------------------------------------------------------- */
 /* Upload ragged per-voxel lists: counts[N], then (idx, val) of all entries concatenated in voxel

@@ -59,7 +59,8 @@ class Model(C.Structure):
     _fields_ = [("nphases", C.c_int32), ("sigma", C.POINTER(C.c_double)), ("mu", C.POINTER(C.c_double)),
                 ("limit", C.POINTER(C.c_double)), ("limiting", C.c_int32), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int32),
-                ("nucleus_volume_factor", C.c_double)]
+                ("nucleus_volume_factor", C.c_double), ("energy_model", C.POINTER(C.c_int32)),
+                ("cubic_eps", C.POINTER(C.c_double)), ("phase_solid", C.POINTER(C.c_int32))]
 
 
 class Stats(C.Structure):
@@ -86,6 +87,7 @@ _SIGS = {
     "opgpu_set_pair_table": (C.c_uint32, [_P, _P, _P]),
     "opgpu_set_pair_hash": (C.c_uint32, [_P, C.c_uint64, C.c_double, C.c_double]),
     "opgpu_set_driving_force": (C.c_uint32, [_P, _P]),
+    "opgpu_set_orientations": (C.c_uint32, [_P, _P]),
     "opgpu_upload_lists": (C.c_uint32, [_P, _P, _P, _P]),
     "opgpu_read_raw": (C.c_uint32, [_P, C.c_char_p]),
     "opgpu_write_raw": (C.c_uint32, [_P, C.c_char_p]),

@@ -54,16 +54,25 @@ class Context:
 
     # ---- parameters
     def set_model(self, sigma, mu, *, limit=None, limiting=True, regularization=1.0, tj_factor=0.0,
-                  consider_nucleus_volume=True, nucleus_volume_factor=1.0):
+                  consider_nucleus_volume=True, nucleus_volume_factor=1.0, energy_model=None, cubic_eps=None,
+                  phase_solid=None):
         sigma = np.ascontiguousarray(np.atleast_2d(sigma), dtype=np.float64)
         mu = np.ascontiguousarray(np.atleast_2d(mu), dtype=np.float64)
         lim = None if limit is None else np.ascontiguousarray(np.atleast_2d(limit), dtype=np.float64)
-        m = Model(nphases=sigma.shape[0], sigma=sigma.ctypes.data_as(C.POINTER(C.c_double)),
-                  mu=mu.ctypes.data_as(C.POINTER(C.c_double)),
-                  limit=lim.ctypes.data_as(C.POINTER(C.c_double)) if lim is not None else None,
-                  limiting=int(limiting), regularization=regularization, tj_factor=tj_factor,
-                  consider_nucleus_volume=int(consider_nucleus_volume), nucleus_volume_factor=nucleus_volume_factor)
+        em = None if energy_model is None else np.ascontiguousarray(energy_model, dtype=np.int32)
+        eps = None if cubic_eps is None else np.ascontiguousarray(cubic_eps, dtype=np.float64)
+        sol = None if phase_solid is None else np.ascontiguousarray(phase_solid, dtype=np.int32)
+        as_ptr = lambda a, t: a.ctypes.data_as(C.POINTER(t)) if a is not None else None  # noqa: E731
+        m = Model(nphases=sigma.shape[0], sigma=as_ptr(sigma, C.c_double), mu=as_ptr(mu, C.c_double),
+                  limit=as_ptr(lim, C.c_double), limiting=int(limiting), regularization=regularization,
+                  tj_factor=tj_factor, consider_nucleus_volume=int(consider_nucleus_volume),
+                  nucleus_volume_factor=nucleus_volume_factor, energy_model=as_ptr(em, C.c_int32),
+                  cubic_eps=as_ptr(eps, C.c_double), phase_solid=as_ptr(sol, C.c_int32))
         _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
+
+    def set_orientations(self, quat):
+        q = None if quat is None else np.ascontiguousarray(quat, dtype=np.float64)
+        _check(lib().opgpu_set_orientations(self.h, ptr(q)), self.h, "set_orientations")
 
     def set_grains(self, ngrains, phase=None, stage=None):
         ph = None if phase is None else np.ascontiguousarray(phase, dtype=np.int32)
@@ -200,9 +209,12 @@ class Context:
     def from_case(cls, case, precision="fp64", k_slots=8, device=0, state=None, threads=0):
         ctx = cls(case.nx, case.ny, case.nz, dx=case.dx, iwidth=case.iwidth, stencil=case.stencil,
                   gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
-        ctx.set_model([[case.sigma]], [[case.mu]], limit=[[case.limit]], limiting=case.limiting,
-                      regularization=case.regularization, tj_factor=case.tj_factor)
-        ctx.set_grains(case.ngrains)
+        ctx.set_model(case.sigma_phase(), case.mu_phase(), limit=case.limit_phase(), limiting=case.limiting,
+                      regularization=case.regularization, tj_factor=case.tj_factor,
+                      energy_model=case.energy_models(), cubic_eps=case.cubic_eps(), phase_solid=case.solid_phase())
+        ctx.set_grains(case.ngrains, phase=case.grain_phase())
+        if case.orientations:
+            ctx.set_orientations(case.quaternions())
         ps = case.pair_sigma()
         if ps is not None:
             ctx.set_pair_table(ps, None)

@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(128) tlm_step_kernel(const __grid_constant__ S
             constexpr int KP = KL * (KL - 1) / 2;
             int16_t gL[KL];
             double vr[KL], lr[KL];
-            const int n = gather_list<double, KL>(p, cnt, gin, vin, nb, v, gL, vr, lr, st);
+            const int n = gather_list<double, KL>(p, cnt, gin, vin, nb, v, gL, vr, lr, nullptr, st);
             Dual val[KL], lap[KL], sg[KP], pv[KP], pos[KL], neg[KL];
             for (int k = 0; k < n; k++)
             {
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(64) adjoint_local_kernel(const __grid_constant
     }
     int16_t g[KL];
     R vr[KL], lr[KL];
-    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, g, vr, lr, st);
+    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, g, vr, lr, nullptr, st);
     double val[KL], lap[KL], lval[KL], llap[KL];
     for (int k = 0; k < n; k++) { val[k] = (double)vr[k]; lap[k] = (double)lr[k]; lval[k] = 0.0; llap[k] = 0.0; }
     int16_t g0[KL];

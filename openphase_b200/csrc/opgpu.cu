@@ -39,6 +39,7 @@ struct opgpu_ctx {
     int8_t *d_gstage = nullptr, *d_exist = nullptr;
     double *d_dg = nullptr, *d_pair_sigma = nullptr, *d_pair_mu = nullptr;
     double* d_dg_pair = nullptr;     // limited driving force per grain pair (G <= kMaxPairTableGrains)
+    double* d_grot = nullptr;        // [G*9] grain rotation matrices (identity unless oriented)
     // checkpoints of the state and the grain records (adjoint rollouts)
     struct Slot {
         uint8_t* cnt = nullptr; int16_t* idx = nullptr; void* val = nullptr;
@@ -282,7 +283,8 @@ void free_grains(opgpu_ctx* c)
 {
     dfree(c->d_vr); dfree(c->d_volume); dfree(c->d_maxvol); dfree(c->d_refvol); dfree(c->d_vol_acc);
     dfree(c->d_gphase); dfree(c->d_gstage); dfree(c->d_exist); dfree(c->d_dg);
-    dfree(c->d_pair_sigma); dfree(c->d_pair_mu); dfree(c->d_dg_pair);
+    dfree(c->d_pair_sigma); dfree(c->d_pair_mu); dfree(c->d_dg_pair); dfree(c->d_grot);
+    c->d_grot = nullptr;
     c->d_vr = c->d_volume = c->d_maxvol = c->d_refvol = c->d_vol_acc = nullptr;
     c->d_gphase = nullptr; c->d_gstage = c->d_exist = nullptr;
     c->d_dg = c->d_pair_sigma = c->d_pair_mu = c->d_dg_pair = nullptr;
@@ -317,6 +319,32 @@ void set_stencils(StepParams& sp, int lap, int grad, double dx)
             sp.lap_d[sp.ns][2] = (signed char)z;
             sp.lap_w[sp.ns] = w / (dx * dx);
             sp.ns++;
+        }
+    }
+    // GradientStencil::Set (include/Containers/GradientStencil.h:132-155) over GradientStencil1D
+    // (:46-56), GradientStencil3D (:82-92) and GradientStencil3D_LB (:108-118): weight c*table/dx
+    sp.ngs = 0;
+    for (int x = -1; x <= 1; ++x)
+    for (int y = -1; y <= 1; ++y)
+    for (int z = -1; z <= 1; ++z)
+    {
+        const int d = (x != 0) + (y != 0) + (z != 0);
+        double t;
+        if (grad == OPGPU_STENCIL_SIMPLE)
+            t = (d == 1) ? 0.5 : 0.0;
+        else if (grad == OPGPU_STENCIL_ISOTROPIC)
+            t = (d == 0) ? 0.0 : (d == 1 ? 1.0 / 4.64 : (d == 2 ? 0.245 / 4.64 : 0.085 / 4.64));
+        else
+            t = (d == 0) ? 0.0 : (d == 1 ? 2.0 / 9.0 : (d == 2 ? 1.0 / 18.0 : 1.0 / 72.0));
+        if (t != 0.0)
+        {
+            sp.gs_d[sp.ngs][0] = (signed char)x;
+            sp.gs_d[sp.ngs][1] = (signed char)y;
+            sp.gs_d[sp.ngs][2] = (signed char)z;
+            sp.gs_w[sp.ngs][0] = x * t / dx;
+            sp.gs_w[sp.ngs][1] = y * t / dx;
+            sp.gs_w[sp.ngs][2] = z * t / dx;
+            sp.ngs++;
         }
     }
     // Candidate discovery by the gradient pass only matters when the Laplacian misses neighbours
@@ -495,12 +523,21 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         sp.sigma_p[q] = m->sigma[q];
         sp.mu_p[q] = m->mu[q];
         const double lim = m->limit ? m->limit[q] : 0.95;   // src/DrivingForce.cpp:161
-        // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor;
-        // the ISO model's MaxEnergy is its Energy (InterfaceEnergyModel.h:82)
-        double allowed = lim * sp.pref_df * m->sigma[q];
+        const int model = m->energy_model ? m->energy_model[q] : 0;
+        if (model < 0 || model > 1) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) or 1 (CUBIC)");
+        sp.emodel[q] = (signed char)model;
+        sp.eps_p[q] = (model == 1 && m->cubic_eps) ? m->cubic_eps[q] : 0.0;
+        // MaxEnergy: Energy for ISO (InterfaceEnergyModel.h:82), Energy*(1 + Epsilon*1.41) for CUBIC
+        // (ReadInputCubic, InterfaceEnergyModel.h:87-94)
+        sp.maxe_p[q] = model == 1 ? m->sigma[q] * (1.0 + sp.eps_p[q] * 1.41) : m->sigma[q];
+        // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor
+        double allowed = lim * sp.pref_df * sp.maxe_p[q];
         allowed *= m->regularization;
         sp.allowed_p[q] = allowed;
     }
+    sp.aniso = 0;
+    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] != 0;
+    for (int a = 0; a < P; a++) sp.solid_p[a] = (signed char)(m->phase_solid ? (m->phase_solid[a] != 0) : 1);
     ctx->nvf = m->nucleus_volume_factor > 0.0 ? m->nucleus_volume_factor : 1.0;
     ctx->model_set = true;
     ctx->dg_pair_dirty = true;
@@ -547,6 +584,12 @@ extern "C" uint32_t opgpu_set_grains(opgpu_ctx* ctx, int32_t ngrains, const int3
     CK(cudaMemcpy(ctx->d_gphase, gp.data(), G * sizeof(int16_t), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_gstage, gs.data(), G * sizeof(int8_t), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_exist, ex.data(), G * sizeof(int8_t), cudaMemcpyHostToDevice));
+    CK(dalloc(&ctx->d_grot, (size_t)G * 9));
+    {
+        std::vector<double> rot((size_t)G * 9, 0.0);
+        for (int g = 0; g < G; g++) { rot[9 * g] = 1.0; rot[9 * g + 4] = 1.0; rot[9 * g + 8] = 1.0; }
+        CK(cudaMemcpy(ctx->d_grot, rot.data(), rot.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     ctx->sp.pair_mode = OPGPU_PAIRS_PHASE;
     ctx->sp.use_dg = 0;
     ctx->initialized = false;
@@ -596,6 +639,39 @@ extern "C" uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG)
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->sp.use_dg = 1;
     ctx->dg_pair_dirty = true;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_orientations(opgpu_ctx* ctx, const double* quat)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_set_orientations: set the grains first")) return r;
+    const int G = ctx->G;
+    std::vector<double> rot((size_t)G * 9, 0.0);
+    for (int g = 0; g < G; g++)
+    {
+        double* R = rot.data() + 9 * (size_t)g;
+        // Quaternion::setRotationMatrix (src/Containers/Quaternion.cpp:78-98) on the quaternion
+        // normalised as Quaternion::normalized (include/Containers/Quaternion.h:304-311)
+        const double qs = quat ? quat[4 * g] : 1.0, q0 = quat ? quat[4 * g + 1] : 0.0;
+        const double q1 = quat ? quat[4 * g + 2] : 0.0, q2 = quat ? quat[4 * g + 3] : 0.0;
+        const double len = std::sqrt(qs * qs + q0 * q0 + q1 * q1 + q2 * q2);
+        if (len < DBL_EPSILON)
+        {
+            R[0] = 1.0; R[4] = 1.0; R[8] = 1.0;
+            continue;
+        }
+        const double S = qs / len, V0 = q0 / len, V1 = q1 / len, V2 = q2 / len;
+        R[0] = 1.0 - 2.0 * (V1 * V1 + V2 * V2);
+        R[1] =       2.0 * (V0 * V1 -  S * V2);
+        R[2] =       2.0 * (V0 * V2 +  S * V1);
+        R[3] =       2.0 * (V0 * V1 +  S * V2);
+        R[4] = 1.0 - 2.0 * (V0 * V0 + V2 * V2);
+        R[5] =       2.0 * (V1 * V2 -  S * V0);
+        R[6] =       2.0 * (V0 * V2 -  S * V1);
+        R[7] =       2.0 * (V1 * V2 +  S * V0);
+        R[8] = 1.0 - 2.0 * (V0 * V0 + V1 * V1);
+    }
+    CK(cudaMemcpy(ctx->d_grot, rot.data(), rot.size() * sizeof(double), cudaMemcpyHostToDevice));
     return OPGPU_OK;
 }
 
@@ -709,6 +785,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
         a.vr = ctx->d_vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
         a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
         a.dg_pair = pair_table ? ctx->d_dg_pair : nullptr;
+        a.grot = ctx->d_grot;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
         a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
@@ -998,6 +1075,7 @@ StepArrays step_arrays(opgpu_ctx* ctx, const uint8_t* cnt_in, const int16_t* idx
     a.vr = vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
     a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
     a.dg_pair = (ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && !ctx->dg_pair_dirty) ? ctx->d_dg_pair : nullptr;
+    a.grot = ctx->d_grot;
     a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
     return a;
 }
@@ -1126,6 +1204,7 @@ extern "C" uint32_t opgpu_adjoint_begin(opgpu_ctx* ctx, const double* dL_dV)
 {
     if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_adjoint_begin: not initialized")) return r;
     if (!dL_dV) return fail(ctx, OPGPU_E_INVALID, "opgpu_adjoint_begin: dL_dV is NULL");
+    if (ctx->sp.aniso) return fail(ctx, OPGPU_E_INVALID, "opgpu_adjoint_begin: anisotropic energy models are not differentiated");
     if (uint32_t r = ensure_adjoint(ctx)) return r;
     const size_t G = (size_t)ctx->G;
     double* d_w = nullptr;
@@ -1193,6 +1272,7 @@ extern "C" uint32_t opgpu_tlm_begin(opgpu_ctx* ctx, const double* dsigma, const 
 {
     if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_tlm_begin: not initialized")) return r;
     if (ctx->fp32) return fail(ctx, OPGPU_E_INVALID, "opgpu_tlm_begin: the tangent-linear model runs the FP64 form");
+    if (ctx->sp.aniso) return fail(ctx, OPGPU_E_INVALID, "opgpu_tlm_begin: anisotropic energy models are not differentiated");
     if (uint32_t r = ensure_tlm(ctx)) return r;
     const size_t G = (size_t)ctx->G;
     if (uint32_t r = upload_upper(ctx, ctx->d_tsig, dsigma)) return r;

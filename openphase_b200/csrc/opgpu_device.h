@@ -67,6 +67,17 @@ struct StepParams {
     double hash_lo, hash_span;
     int ngrains;
     int use_dg;
+    // anisotropic interface energy (InterfaceProperties::SetSR, src/InterfaceProperties.cpp:617-673):
+    // per phase pair the model (0 ISO, 1 CUBIC), its epsilon and MaxEnergy; per phase solid (1) or
+    // liquid (0); the gradient stencil in GradientStencil::Set order with its weights per axis
+    int aniso;
+    signed char emodel[kMaxPhases * kMaxPhases];
+    double eps_p[kMaxPhases * kMaxPhases];
+    double maxe_p[kMaxPhases * kMaxPhases];
+    signed char solid_p[kMaxPhases];
+    int ngs;
+    signed char gs_d[27][3];
+    double gs_w[27][3];
 };
 
 struct StepArrays {
@@ -83,6 +94,7 @@ struct StepArrays {
     const double* pair_sigma;  // [G*G] or null
     const double* pair_mu;     // [G*G] or null
     const double* dg_pair;     // [G*G] limited driving force per grain pair, or null (evaluated in place)
+    const double* grot;        // [G*9] grain rotation matrices (row-major), for anisotropic energies
     double* vol_acc;           // [G] volume accumulator of the output state (zeroed by the caller)
     uint32_t* status;          // soft status bits
     unsigned long long* counters;  // kNumCounters

@@ -97,7 +97,84 @@ struct ListScratch {
     double* pos;     // [KL] positive increments / upper limits
     double* neg;     // [KL] negative increments / lower limits
     int stride;
+    const R* grad;   // [KL*3] gradients, entry k at grad[3k..3k+2] (anisotropic energies), or null
 };
+
+// InterfaceOrientation (src/InterfaceProperties.cpp:39-45): -grad normalised (dVector3::normalize,
+// include/Containers/dVector3.h:301-316), rotated back with the transposed RotationMatrix
+// (include/Containers/MatrixVectorOperators.h:43-52).
+__device__ __forceinline__ void interface_orientation(const double* g3, const double* R, double* out)
+{
+    double n0 = g3[0] * (-1.0), n1 = g3[1] * (-1.0), n2 = g3[2] * (-1.0);
+    const double norm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    if (norm > DBL_EPSILON)
+    {
+        const double inv = 1.0 / norm;
+        n0 *= inv; n1 *= inv; n2 *= inv;
+    }
+    else
+    {
+        n0 = 0.0; n1 = 0.0; n2 = 0.0;
+    }
+    for (int i = 0; i < 3; i++)
+    {
+        double t = 0.0;
+        t += R[i] * n0;
+        t += R[3 + i] * n1;
+        t += R[6 + i] * n2;
+        out[i] = t;
+    }
+}
+
+// InterfaceEnergyModel::Calculate, CUBIC (include/InterfaceProperties/InterfaceEnergyModel.h:325-345).
+__device__ __forceinline__ double cubic_energy(double energy, double eps, const double* n)
+{
+    return energy * (1.0 + eps * (1.5 - 2.5 * (pow(n[0], 4.0) + pow(n[1], 4.0) + pow(n[2], 4.0))));
+}
+
+// The interface energy of the pair (i, j) of a voxel's list as InterfaceProperties::SetSR stores it
+// (src/InterfaceProperties.cpp:617-673): the ISO value, or the anisotropic model averaged over the
+// solid grains' interface orientations with weights |phi(1 - phi)| (MaxEnergy when no weight counts).
+template <class R>
+__device__ __forceinline__ double voxel_energy(const StepParams& p, const StepArrays& a, const ListScratch<R>& sc,
+                                               int i, int j)
+{
+    const int S = sc.stride;
+    const int gi = sc.g[i * S], gj = sc.g[j * S];
+    const int pA = a.gphase[gi], pB = a.gphase[gj];
+    const int q = pA * p.nphases + pB;
+    if (p.emodel[q] == 0) return pair_energy(p, a, gi, gj);
+    double loc = 0.0, wA = 0.0, wB = 0.0;
+    if (p.solid_p[pA])
+    {
+        const double v = (double)sc.val[i * S];
+        wA = fabs(v * (1.0 - v));
+        if (wA > DBL_EPSILON)
+        {
+            const double g3[3] = {(double)sc.grad[(3 * i) * S], (double)sc.grad[(3 * i + 1) * S], (double)sc.grad[(3 * i + 2) * S]};
+            double n[3];
+            interface_orientation(g3, a.grot + 9 * (long long)gi, n);
+            loc += cubic_energy(p.sigma_p[q], p.eps_p[q], n) * wA;
+        }
+        else wA = 0.0;
+    }
+    if (p.solid_p[pB])
+    {
+        const double v = (double)sc.val[j * S];
+        wB = fabs(v * (1.0 - v));
+        if (wB > DBL_EPSILON)
+        {
+            const double g3[3] = {(double)sc.grad[(3 * j) * S], (double)sc.grad[(3 * j + 1) * S], (double)sc.grad[(3 * j + 2) * S]};
+            double n[3];
+            interface_orientation(g3, a.grot + 9 * (long long)gj, n);
+            loc += cubic_energy(p.sigma_p[q], p.eps_p[q], n) * wB;
+        }
+        else wB = 0.0;
+    }
+    if (wA + wB > DBL_EPSILON) loc /= wA + wB;
+    else loc = p.maxe_p[q];
+    return loc;
+}
 
 // Stages 2-5 for a list of n fields (own fields first, then candidates, as CalculateDerivativesSR
 // leaves them) with their Laplacians.  Leaves the new record (the fields that survive finalize, in
@@ -127,7 +204,8 @@ __device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& 
     }
     const R norm_1 = (R)(1.0 / localN);
     for (int i = 0; i < n; i++)
-        for (int j = i + 1; j < n; j++) SG_(pair_pos(i, j, n)) = (R)pair_energy(p, a, G_(i), G_(j));
+        for (int j = i + 1; j < n; j++)
+            SG_(pair_pos(i, j, n)) = (R)(p.aniso ? voxel_energy<R>(p, a, sc, i, j) : pair_energy(p, a, G_(i), G_(j)));
     const R pref = (R)p.pref_do;
     for (int i = 0; i < n; i++)
     {
@@ -385,7 +463,7 @@ template <class R, int KL>
 __device__ __forceinline__ int gather_list(const StepParams& p, const uint8_t* __restrict__ cnt,
                                            const int16_t* __restrict__ gin, const R* __restrict__ vin,
                                            const Neighbourhood& nb, long long v, int16_t* gL, R* val, R* lap,
-                                           uint32_t& st)
+                                           R* grad, uint32_t& st)
 {
     const long long N = p.n;
     const int c = cnt[v];
@@ -438,6 +516,35 @@ __device__ __forceinline__ int gather_list(const StepParams& p, const uint8_t* _
             }
         }
     }
+    // gradients of every list entry (anisotropic energies only), summed in gradient-stencil order
+    if (p.aniso && grad)
+    {
+        for (int k = 0; k < 3 * n; k++) grad[k] = R(0);
+        for (int q = 0; q < p.ngs; q++)
+        {
+            const long long u = nb.at(p.gs_d[q][0], p.gs_d[q][1], p.gs_d[q][2]);
+            const int cu = cnt[u];
+            for (int s = 0; s < cu; s++)
+            {
+                const R phi = vin[s * N + u];
+                if (phi != R(0))
+                {
+                    const int g = gin[s * N + u];
+                    int f = 0;
+                    while (f < n && gL[f] != g) f++;
+                    if (f < n)
+                    {
+                        const R gx = (R)p.gs_w[q][0] * phi;
+                        const R gy = (R)p.gs_w[q][1] * phi;
+                        const R gz = (R)p.gs_w[q][2] * phi;
+                        grad[3 * f] += gx;
+                        grad[3 * f + 1] += gy;
+                        grad[3 * f + 2] += gz;
+                    }
+                }
+            }
+        }
+    }
     return n;
 }
 
@@ -482,8 +589,9 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     int16_t gL[KL];
     R val[KL], lap[KL], sg[KP];
     double pv[KP], pos[KL], neg[KL];
-    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, st);
-    const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1};
+    R grad[3 * KL];
+    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, grad, st);
+    const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1, grad};
     int m = list_step<R>(p, a, sc, n, flag, st);
     if (m > KS) { st |= kStOverflowK; m = KS; }
     a.cnt_out[v] = (uint8_t)m;

@@ -791,8 +791,9 @@ template <class R>
 int launch_step(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
                 LaunchInfo* info)
 {
-    if (variant == kVariantGeneric)
+    if (variant == kVariantGeneric || p.aniso)
     {
+        // anisotropic energies need the gradients of every list entry: the general path only
         if (info) info->kernels += 1;
         return launch_step_generic<R>(p, a, k_slots, stream);
     }
