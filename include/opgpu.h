@@ -226,6 +226,29 @@ uint32_t opgpu_tlm_step(opgpu_ctx* ctx, double dt, int32_t nsteps);
 /* Tangent of the grain volumes of the current state, dV[G]. */
 uint32_t opgpu_tlm_volumes(opgpu_ctx* ctx, double* dV);
 
+/* ---- slab decomposition --------------------------------------------------------------------- */
+/* A rank holds an x-slab of the global grid plus one halo plane on each side (local nx = slab + 2);
+ * before each step the halo planes are refreshed from the neighbouring ranks, and the grain
+ * volumes are summed over the slab only and all-reduced across ranks.  The reference does the
+ * same with MPI (halo cells, include/BoundaryConditions.h:2747-2854; volume all-reduce,
+ * src/PhaseField.cpp:854-892); these entry points have no direct counterpart. */
+/* Only planes x0 <= x < x1 count in the grain volumes (call before uploading the state). */
+uint32_t opgpu_set_volume_window(opgpu_ctx* ctx, int32_t x0, int32_t x1);
+/* Bytes of one packed x-plane: ny*nz count bytes, then K index planes (int16), then K value planes. */
+int64_t  opgpu_plane_bytes(opgpu_ctx* ctx);
+/* Copy x-plane x of the current state to / from a device buffer of opgpu_plane_bytes bytes. */
+uint32_t opgpu_pack_plane(opgpu_ctx* ctx, int32_t x, void* dev_buf);
+uint32_t opgpu_unpack_plane(opgpu_ctx* ctx, int32_t x, const void* dev_buf);
+/* Recompute the grain-volume accumulator from the window planes of the current state. */
+uint32_t opgpu_volume_recount(opgpu_ctx* ctx);
+/* One step whose grain update is deferred: the window's volume sums stay in the accumulator. */
+uint32_t opgpu_step_partial(opgpu_ctx* ctx, double dt);
+/* Copy the accumulator (G doubles) to a device buffer (for the all-reduce). */
+uint32_t opgpu_volume_accumulator(opgpu_ctx* ctx, double* dev_dst);
+/* Set the accumulator from a device buffer (the all-reduced sums) and run the grain update; with
+ * initial != 0 it is the update of FinalizeInitialization (MAXVolume and Exist restart). */
+uint32_t opgpu_step_complete(opgpu_ctx* ctx, const double* dev_src, int32_t initial);
+
 /* ---- host-side initial states (no GPU needed) ---------------------------------------------- */
 /* Counter-based generator shared by host and device: SplitMix64 (Steele, Lea, Flood 2014) over
  * the key (seed, stream, a, b); uniform in [0,1) with 53 bits. */

@@ -114,6 +114,14 @@ _SIGS = {
     "opgpu_tlm_begin": (C.c_uint32, [_P, _P, _P, _P]),
     "opgpu_tlm_step": (C.c_uint32, [_P, C.c_double, C.c_int32]),
     "opgpu_tlm_volumes": (C.c_uint32, [_P, _P]),
+    "opgpu_set_volume_window": (C.c_uint32, [_P, C.c_int32, C.c_int32]),
+    "opgpu_plane_bytes": (C.c_int64, [_P]),
+    "opgpu_pack_plane": (C.c_uint32, [_P, C.c_int32, _P]),
+    "opgpu_unpack_plane": (C.c_uint32, [_P, C.c_int32, _P]),
+    "opgpu_volume_recount": (C.c_uint32, [_P]),
+    "opgpu_step_partial": (C.c_uint32, [_P, C.c_double]),
+    "opgpu_volume_accumulator": (C.c_uint32, [_P, _P]),
+    "opgpu_step_complete": (C.c_uint32, [_P, _P, C.c_int32]),
     "opgpu_uniform": (C.c_double, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
     "opgpu_voronoi_owner_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                               C.c_int32, _P]),

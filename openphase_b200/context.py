@@ -204,6 +204,31 @@ class Context:
         _check(lib().opgpu_tlm_volumes(self.h, ptr(dV)), self.h, "tlm_volumes")
         return dV
 
+    # ---- slab decomposition (device buffers are passed as raw device addresses)
+    def set_volume_window(self, x0: int, x1: int):
+        _check(lib().opgpu_set_volume_window(self.h, int(x0), int(x1)), self.h, "set_volume_window")
+
+    def plane_bytes(self) -> int:
+        return int(lib().opgpu_plane_bytes(self.h))
+
+    def pack_plane(self, x: int, dev_ptr: int):
+        _check(lib().opgpu_pack_plane(self.h, int(x), C.c_void_p(dev_ptr)), self.h, "pack_plane")
+
+    def unpack_plane(self, x: int, dev_ptr: int):
+        _check(lib().opgpu_unpack_plane(self.h, int(x), C.c_void_p(dev_ptr)), self.h, "unpack_plane")
+
+    def volume_recount(self):
+        _check(lib().opgpu_volume_recount(self.h), self.h, "volume_recount")
+
+    def step_partial(self, dt: float) -> int:
+        return _check(lib().opgpu_step_partial(self.h, float(dt)), self.h, "step_partial")
+
+    def volume_accumulator(self, dev_ptr: int):
+        _check(lib().opgpu_volume_accumulator(self.h, C.c_void_p(dev_ptr)), self.h, "volume_accumulator")
+
+    def step_complete(self, dev_ptr: int, initial: bool = False) -> int:
+        return _check(lib().opgpu_step_complete(self.h, C.c_void_p(dev_ptr), int(initial)), self.h, "step_complete")
+
     # ---- convenience
     @classmethod
     def from_case(cls, case, precision="fp64", k_slots=8, device=0, state=None, threads=0):

@@ -461,6 +461,7 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
     cudaMemset(ctx->d_counters, 0, kNumCounters * sizeof(unsigned long long));
     StepParams& sp = ctx->sp;
     sp.nx = g.nx; sp.ny = g.ny; sp.nz = g.nz; sp.n = ctx->n;
+    sp.vol_x0 = 0; sp.vol_x1 = g.nx;
     set_stencils(sp, g.laplacian_stencil, g.gradient_stencil, g.dx);
     const double Eta = g.iwidth * g.dx;                 // src/GridParameters.cpp:256
     sp.pref_do = kPi * kPi / (Eta * Eta);               // src/DoubleObstacle.cpp:504
@@ -760,7 +761,7 @@ extern "C" uint32_t opgpu_finalize_initialization(opgpu_ctx* ctx)
     return st & OPGPU_SOFT_MASK;
 }
 
-static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
+static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partial = false)
 {
     if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_step: call opgpu_finalize_initialization first")) return r;
     if (nsteps < 0 || !(dt > 0.0)) return fail(ctx, OPGPU_E_INVALID, "opgpu_step: dt > 0 and nsteps >= 0 required");
@@ -817,10 +818,14 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps)
             CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used + 2], ctx->stream));
             ctx->ev_used++;
         }
-        ctx->kernel_launches += info.kernels + 1;   // + grains_update_kernel
-        grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
-            ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 1);
-        CK(cudaGetLastError());
+        ctx->kernel_launches += info.kernels;
+        if (!partial)
+        {
+            grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
+                ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, 1);
+            CK(cudaGetLastError());
+            ctx->kernel_launches++;
+        }
         ctx->cur = out;
     }
     return OPGPU_OK;
@@ -1322,4 +1327,114 @@ extern "C" uint32_t opgpu_tlm_volumes(opgpu_ctx* ctx, double* dV)
     CK(cudaMemcpyAsync(dV, ctx->d_tvol, (size_t)ctx->G * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return OPGPU_OK;
+}
+
+// ---- slab decomposition support (no reference counterpart: the reference exchanges halo cells with
+// MPI, include/BoundaryConditions.h:2747-2854, and all-reduces the grain volumes,
+// src/PhaseField.cpp:854-892) -------------------------------------------------------------------
+namespace {
+
+__global__ void grains_reset_kernel(int G, double* maxv, int8_t* exist)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < G) { maxv[g] = 0.0; exist[g] = 1; }
+}
+
+}  // namespace
+
+extern "C" uint32_t opgpu_set_volume_window(opgpu_ctx* ctx, int32_t x0, int32_t x1)
+{
+    if (uint32_t r = require(ctx, true, "")) return r;
+    if (x0 < 0 || x1 > ctx->grid.nx || x0 >= x1)
+        return fail(ctx, OPGPU_E_INVALID, "opgpu_set_volume_window: need 0 <= x0 < x1 <= nx");
+    ctx->sp.vol_x0 = x0;
+    ctx->sp.vol_x1 = x1;
+    return OPGPU_OK;
+}
+
+extern "C" int64_t opgpu_plane_bytes(opgpu_ctx* ctx)
+{
+    if (!ctx) return 0;
+    const long long P = (long long)ctx->grid.ny * ctx->grid.nz;
+    return P * (1 + (long long)ctx->K * (2 + (long long)ctx->rsz));
+}
+
+static uint32_t plane_copy(opgpu_ctx* ctx, int32_t x, void* buf, bool pack)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded, "plane copy: no state")) return r;
+    if (x < 0 || x >= ctx->grid.nx || !buf) return fail(ctx, OPGPU_E_INVALID, "plane copy: x out of range or NULL buffer");
+    const size_t P = (size_t)ctx->grid.ny * ctx->grid.nz, N = (size_t)ctx->n, K = (size_t)ctx->K;
+    unsigned char* b = static_cast<unsigned char*>(buf);
+    uint8_t* c = ctx->cnt[ctx->cur] + (size_t)x * P;
+    unsigned char* i = reinterpret_cast<unsigned char*>(ctx->idx[ctx->cur] + (size_t)x * P);
+    unsigned char* v = static_cast<unsigned char*>(ctx->val[ctx->cur]) + (size_t)x * P * ctx->rsz;
+    unsigned char* bi = b + P;
+    unsigned char* bv = bi + P * K * 2;
+    const cudaMemcpyKind kind = cudaMemcpyDeviceToDevice;
+    if (pack)
+    {
+        CK(cudaMemcpyAsync(b, c, P, kind, ctx->stream));
+        CK(cudaMemcpy2DAsync(bi, P * 2, i, N * 2, P * 2, K, kind, ctx->stream));
+        CK(cudaMemcpy2DAsync(bv, P * ctx->rsz, v, N * ctx->rsz, P * ctx->rsz, K, kind, ctx->stream));
+    }
+    else
+    {
+        CK(cudaMemcpyAsync(c, b, P, kind, ctx->stream));
+        CK(cudaMemcpy2DAsync(i, N * 2, bi, P * 2, P * 2, K, kind, ctx->stream));
+        CK(cudaMemcpy2DAsync(v, N * ctx->rsz, bv, P * ctx->rsz, P * ctx->rsz, K, kind, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_pack_plane(opgpu_ctx* ctx, int32_t x, void* dev_buf) { return plane_copy(ctx, x, dev_buf, true); }
+extern "C" uint32_t opgpu_unpack_plane(opgpu_ctx* ctx, int32_t x, const void* dev_buf)
+{
+    return plane_copy(ctx, x, const_cast<void*>(dev_buf), false);
+}
+
+extern "C" uint32_t opgpu_volume_recount(opgpu_ctx* ctx)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded && ctx->G > 0, "opgpu_volume_recount: no state")) return r;
+    CK(cudaMemsetAsync(ctx->d_vol_acc, 0, (size_t)ctx->G * sizeof(double), ctx->stream));
+    if (launch_volume_recount(ctx->sp, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur], ctx->fp32,
+                              ctx->d_vol_acc, ctx->stream))
+        return fail(ctx, OPGPU_E_CUDA, "opgpu_volume_recount: launch");
+    ctx->kernel_launches++;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_step_partial(opgpu_ctx* ctx, double dt)
+{
+    if (uint32_t r = enqueue_steps(ctx, dt, 1, true)) return r;
+    return opgpu_sync(ctx);
+}
+
+extern "C" uint32_t opgpu_volume_accumulator(opgpu_ctx* ctx, double* dev_dst)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_volume_accumulator: no grains")) return r;
+    if (!dev_dst) return fail(ctx, OPGPU_E_INVALID, "opgpu_volume_accumulator: NULL buffer");
+    CK(cudaMemcpyAsync(dev_dst, ctx->d_vol_acc, (size_t)ctx->G * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_step_complete(opgpu_ctx* ctx, const double* dev_src, int32_t initial)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_step_complete: no grains")) return r;
+    if (!dev_src) return fail(ctx, OPGPU_E_INVALID, "opgpu_step_complete: NULL buffer");
+    CK(cudaMemcpyAsync(ctx->d_vol_acc, dev_src, (size_t)ctx->G * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (initial)
+    {
+        grains_reset_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_maxvol, ctx->d_exist);
+        CK(cudaGetLastError());
+    }
+    grains_update_kernel<<<grid_for(ctx->G, 256), 256, 0, ctx->stream>>>(ctx->G, ctx->d_vol_acc, ctx->d_volume,
+        ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, initial ? 0 : 1);
+    CK(cudaGetLastError());
+    ctx->kernel_launches += initial ? 2 : 1;
+    const uint32_t st = read_status(ctx);
+    if (st & OPGPU_E_CUDA) return st;
+    return st & OPGPU_SOFT_MASK;
 }

@@ -78,7 +78,18 @@ struct StepParams {
     int ngs;
     signed char gs_d[27][3];
     double gs_w[27][3];
+    // x-planes [vol_x0, vol_x1) count in the grain volumes (all planes unless a slab of a larger
+    // grid: its halo planes are excluded)
+    int vol_x0, vol_x1;
 };
+
+// Whether voxel v lies in the planes that count in the grain volumes.
+__device__ __forceinline__ bool in_volume_window(const StepParams& p, long long v)
+{
+    if (p.vol_x0 == 0 && p.vol_x1 == p.nx) return true;
+    const int x = (int)(v / ((long long)p.ny * p.nz));
+    return x >= p.vol_x0 && x < p.vol_x1;
+}
 
 struct StepArrays {
     const uint8_t* cnt_in;
@@ -148,5 +159,8 @@ int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int v
 // Fill out[a*G+b] with the limited driving force of every grain pair (defined in step_f64.cu, so
 // that it is compiled exactly like the in-place evaluation of the FP64 form).
 int launch_dg_pair(const StepParams& p, const double* dg, const int16_t* gphase, double* out, void* stream);
+// Add the volumes of the window planes of a state to vol_acc (defined in step_f64.cu).
+int launch_volume_recount(const StepParams& p, const uint8_t* cnt, const int16_t* idx, const void* val, int fp32,
+                          double* vol_acc, void* stream);
 
 }  // namespace opgpu

@@ -578,7 +578,7 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
             const R phi = vin[s * N + v];
             a.idx_out[s * N + v] = (int16_t)g;
             vout[s * N + v] = phi;
-            vol_insert_n(s_key, s_sum, nslots, a.vol_acc, g, (double)phi);
+            if (in_volume_window(p, v)) vol_insert_n(s_key, s_sum, nslots, a.vol_acc, g, (double)phi);
         }
         eout = c;
         return;
@@ -599,7 +599,7 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     {
         a.idx_out[i * N + v] = gL[i];
         vout[i * N + v] = val[i];
-        vol_insert_n(s_key, s_sum, nslots, a.vol_acc, gL[i], (double)val[i]);
+        if (in_volume_window(p, v)) vol_insert_n(s_key, s_sum, nslots, a.vol_acc, gL[i], (double)val[i]);
     }
     eout = m;
 }

@@ -386,7 +386,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
                 const R phi = static_cast<const R*>(a.val_in)[s * N + v];
                 a.idx_out[s * N + v] = (int16_t)g;
                 vout[s * N + v] = phi;
-                vol_insert_n(S.vol_key, S.vol_sum, kClassifyVolSlots, a.vol_acc, g, (double)phi);
+                if (in_volume_window(p, v)) vol_insert_n(S.vol_key, S.vol_sum, kClassifyVolSlots, a.vol_acc, g, (double)phi);
             }
             eout += c;
             continue;
@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
                 if (!isfinite((double)w)) st |= kStNonFinite;
                 a.idx_out[pos * N_ + v] = (int16_t)g[i];
                 vout[pos * N_ + v] = w;
-                vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, g[i], (double)w);
+                if (in_volume_window(p, v)) vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, g[i], (double)w);
                 pos++;
             }
         }
