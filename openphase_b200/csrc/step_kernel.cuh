@@ -467,6 +467,12 @@ __device__ __forceinline__ int gather_list(const StepParams& p, const uint8_t* _
 {
     const long long N = p.n;
     const int c = cnt[v];
+    if (c > KL)
+    {
+        // more stored fields than the list holds: nothing is written; the caller defers or reports
+        st |= kStOverflowList;
+        return 0;
+    }
     int n = 0;
     for (int s = 0; s < c; s++)
     {
@@ -552,10 +558,14 @@ __device__ __forceinline__ int gather_list(const StepParams& p, const uint8_t* _
 // working arrays in local memory (capacity KL fields).  This is the general path: the full-grid
 // kernel below and the overflow kernel of the tiled step (lists longer than the tiled kernel's
 // capacity) both run it.
-template <class R, int KS, int KL>
+// ANISO: gradients for anisotropic energies.  With `defer` (a worklist with its counter and
+// capacity), a voxel whose list exceeds KL is appended there, untouched, for a larger-capacity pass.
+template <class R, int KS, int KL, bool ANISO>
 __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const StepArrays& a, long long v,
                                                    int* s_key, double* s_sum, int nslots, unsigned& wide,
-                                                   unsigned& ein, unsigned& eout, uint32_t& st, bool count_in)
+                                                   unsigned& ein, unsigned& eout, uint32_t& st, bool count_in,
+                                                   int* defer = nullptr, unsigned* defer_count = nullptr,
+                                                   unsigned defer_cap = 0)
 {
     const long long N = p.n;
     const uint8_t* __restrict__ cnt = a.cnt_in;
@@ -589,9 +599,19 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     int16_t gL[KL];
     R val[KL], lap[KL], sg[KP];
     double pv[KP], pos[KL], neg[KL];
-    R grad[3 * KL];
-    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, grad, st);
-    const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1, grad};
+    R grad[ANISO ? 3 * KL : 1];
+    uint32_t st_list = 0;
+    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, ANISO ? grad : nullptr, st_list);
+    if ((st_list & kStOverflowList) && defer)
+    {
+        const unsigned slot = atomicAdd(defer_count, 1u);
+        if (slot < defer_cap) defer[slot] = (int)v;
+        else st |= kStOverflowList;
+        wide = 0;
+        return;
+    }
+    st |= st_list;
+    const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1, ANISO ? grad : nullptr};
     int m = list_step<R>(p, a, sc, n, flag, st);
     if (m > KS) { st |= kStOverflowK; m = KS; }
     a.cnt_out[v] = (uint8_t)m;
@@ -631,7 +651,7 @@ __device__ __forceinline__ void flush_block(const StepArrays& a, unsigned wide, 
         atomicAdd(&a.counters[t == 0 ? kCntWide : (t == 1 ? kCntEntriesIn : kCntEntriesOut)], s_cnt[t]);
 }
 
-template <class R, int KS, int KL>
+template <class R, int KS, int KL, bool ANISO>
 __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepParams p, const StepArrays a)
 {
     __shared__ int s_key[kVolSlots];
@@ -644,7 +664,7 @@ __global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepP
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned wide = 0, ein = 0, eout = 0;
     uint32_t st = 0;
-    if (v < p.n) voxel_step_generic<R, KS, KL>(p, a, v, s_key, s_sum, kVolSlots, wide, ein, eout, st, true);
+    if (v < p.n) voxel_step_generic<R, KS, KL, ANISO>(p, a, v, s_key, s_sum, kVolSlots, wide, ein, eout, st, true);
     flush_block(a, wide, ein, eout, st, s_cnt, s_key, s_sum, kVolSlots, threadIdx.x, blockDim.x);
 }
 
@@ -654,11 +674,14 @@ int launch_step_generic(const StepParams& p, const StepArrays& a, int k_slots, v
     const int threads = 256;
     const long long blocks = (p.n + threads - 1) / threads;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    switch (k_slots)
+    switch (k_slots * 2 + (p.aniso ? 1 : 0))
     {
-        case 8:  step_kernel<R, 8, 16><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
-        case 12: step_kernel<R, 12, 20><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
-        case 16: step_kernel<R, 16, 24><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
+        case 16: step_kernel<R, 8, 16, false><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
+        case 17: step_kernel<R, 8, 16, true><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
+        case 24: step_kernel<R, 12, 20, false><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
+        case 25: step_kernel<R, 12, 20, true><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
+        case 32: step_kernel<R, 16, 24, false><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
+        case 33: step_kernel<R, 16, 24, true><<<(unsigned)blocks, threads, 0, s>>>(p, a); break;
         default: return -1;
     }
     return (int)cudaGetLastError();

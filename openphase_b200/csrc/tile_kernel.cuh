@@ -724,7 +724,9 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
 // Voxels whose field + candidate list exceeds the split kernels' capacity, through the general
 // per-voxel path (grid-stride over the worklist; the classify kernel already counted them as wide
 // and counted their input entries).
-template <class R, int KS, int KL>
+// TIER 1 takes the classify kernel's worklist with a list capacity of KL and defers longer lists to
+// the second worklist; TIER 2 takes that one with the large capacity.
+template <class R, int KS, int KL, int TIER>
 __global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constant__ StepParams p, const StepArrays a)
 {
     __shared__ int s_key[kVolSlots];
@@ -733,14 +735,20 @@ __global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constan
     for (int i = threadIdx.x; i < kVolSlots; i += blockDim.x) { s_key[i] = -1; s_sum[i] = 0.0; }
     if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0ull;
     __syncthreads();
-    const unsigned total = min(*a.slow_count, a.slow_cap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters[kCntGeneralLast], (unsigned long long)total);
+    const int* list = TIER == 1 ? a.slow_list : a.slow2_list;
+    const unsigned total = min(TIER == 1 ? *a.slow_count : *a.slow2_count, a.slow_cap);
+    if (TIER == 1 && blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(&a.counters[kCntGeneralLast], (unsigned long long)total);
     uint32_t st = 0;
     unsigned eo_sum = 0;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
     {
         unsigned wide = 0, ein = 0, eout = 0;
-        voxel_step_generic<R, KS, KL>(p, a, a.slow_list[i], s_key, s_sum, kVolSlots, wide, ein, eout, st, false);
+        if (TIER == 1)
+            voxel_step_generic<R, KS, KL, false>(p, a, list[i], s_key, s_sum, kVolSlots, wide, ein, eout, st, false,
+                                                 a.slow2_list, a.slow2_count, a.slow_cap);
+        else
+            voxel_step_generic<R, KS, KL, false>(p, a, list[i], s_key, s_sum, kVolSlots, wide, ein, eout, st, false);
         eo_sum += eout;
     }
     flush_block(a, 0u, 0u, eo_sum, st, s_cnt, s_key, s_sum, kVolSlots, threadIdx.x, blockDim.x);
@@ -760,6 +768,8 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     if (e != cudaSuccess) return (int)e;
     e = cudaMemsetAsync(a.slow_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return (int)e;
+    e = cudaMemsetAsync(a.slow2_count, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return (int)e;
     kern<<<dim3(gz, gy, gx), dim3(32, kTileTY), smem, s>>>(p, a, xchunk);
     if (info && info->after_classify)
     {
@@ -773,9 +783,11 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     list_compute_kernel<R, 6, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 7, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a);
-    // one warp per SM: the general path's per-thread working arrays then stay in L1
-    overflow_step_kernel<R, KS, KL><<<148, 32, 0, s>>>(p, a);
-    if (info) info->kernels += 9;
+    // general path: lists up to 12 fields with four warps per SM, then the longer ones with one
+    // warp per SM (the per-thread working arrays then stay in L1)
+    overflow_step_kernel<R, KS, 12, 1><<<148, 128, 0, s>>>(p, a);
+    overflow_step_kernel<R, KS, KL, 2><<<148, 32, 0, s>>>(p, a);
+    if (info) info->kernels += 10;
     return (int)cudaGetLastError();
 }
 
