@@ -336,19 +336,21 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     prefetch_counts<TY>(p, a, x0 == 0 ? nx - 1 : x0 - 1, y0, z0, t, cr);
     __syncthreads();
 
-    load_plane(p, a, S, 0, x0 == 0 ? nx - 1 : x0 - 1, -1, y0, z0, t, cr);
-    __syncthreads();
-    load_plane(p, a, S, 1, x0, 0, y0, z0, t, cr);
     const int rec0 = (ty + 1) * kC + (tz + 1);
 
-    for (int x = x0; x < x1; x++)
+    // plane x0-1+j goes to ring slot j%3 at window position j-1; once three planes are in, the
+    // centre plane x = x0+j-2 is processed (one call site of the plane loader keeps the code small)
+    const int nj = (x1 - x0) + 2;
+    for (int j = 0; j < nj; j++)
     {
-        const int xi = x - x0;
-        const int sl0 = xi % 3, sl1 = (xi + 1) % 3, sl2 = (xi + 2) % 3;
+        int xp = x0 - 1 + j;
+        xp = xp < 0 ? xp + nx : (xp >= nx ? xp - nx : xp);
+        if (j > 0) __syncthreads();
+        load_plane(p, a, S, j % 3, xp, j - 1, y0, z0, t, cr);
         __syncthreads();
-        load_plane(p, a, S, sl2, x == nx - 1 ? 0 : x + 1, xi + 1, y0, z0, t, cr);
-        __syncthreads();
-        if (!inside) continue;
+        if (j < 2 || !inside) continue;
+        const int x = x0 + j - 2;
+        const int sl0 = (j - 2) % 3, sl1 = (j - 1) % 3, sl2 = j % 3;
         const bool window_bad = S.bad[0] | S.bad[1] | S.bad[2];
         const long long v = (long long)x * plane + (long long)y * nz + z;
 
@@ -359,20 +361,34 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         int n = c;
         bool over = window_bad || c > kListCap;
         if (!over) ls = S.slotl[sl1][rec0];   // c <= kListCap entries, unused nibbles are zero
-        uint32_t seen = S.word[sl1][rec0] & 0xFFFFu;
+        const uint32_t own = S.word[sl1][rec0] & 0xFFFFu;
+        uint32_t seen = own;
         uint32_t multi = 0;
 #pragma unroll
         for (int q = 0; q < 27; q++)
         {
             const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
             const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
-            const uint32_t w = S.word[pl][r];
-            multi |= w;
-            if (NS == 27 && q != 13)
+            multi |= S.word[pl][r];
+        }
+        // candidates in the reference's order: new grains of each neighbour in stencil order and
+        // neighbour-list order (a rolled loop, entered only when some neighbour holds a new grain)
+        if (NS == 27 && !over && ((multi & 0xFFFFu) & ~own))
+        {
+#pragma unroll 1
+            for (int q = 0; q < 27; q++)
             {
-                const uint32_t fresh = w & 0xFFFFu & ~seen;
-                if (fresh && !over) append_fresh(S, pl, r, fresh, ls, n, over);
-                seen |= w & 0xFFFFu;
+                if (q == 13) continue;
+                const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
+                const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
+                const uint32_t w = S.word[pl][r] & 0xFFFFu;
+                const uint32_t fresh = w & ~seen;
+                if (fresh)
+                {
+                    append_fresh(S, pl, r, fresh, ls, n, over);
+                    if (over) break;
+                }
+                seen |= w;
             }
         }
         const int flag = c > 1 ? 2 : ((multi >> 31) ? 1 : 0);
