@@ -450,7 +450,7 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
         int xchunk = 0, gz = 0, gy = 0, gx = 0;
         tiled_geometry(g.nx, g.ny, g.nz, &xchunk, &gz, &gy, &gx);
         const long long nblocks = (long long)gz * gy * gx;
-        ctx->slice = 32 * kTileRows * xchunk;
+        ctx->slice = kTileCols * kTileRows * xchunk;
         ctx->bucket_cap = nblocks * ctx->slice;
         ctx->wl_slice = (long long)ctx->slice * work_record_bytes(kListCap, (int)ctx->rsz);
         if (dalloc(&ctx->d_wl, (size_t)(nblocks * ctx->wl_slice)) != cudaSuccess) return bail(OPGPU_E_CUDA);

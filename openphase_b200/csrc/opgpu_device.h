@@ -127,14 +127,15 @@ struct StepArrays {
 };
 
 constexpr int kListCap = 8;    // list capacity of the split kernels (longer lists: overflow worklist)
-constexpr int kTileRows = 4;   // tile rows of the classify kernel (tiles of 32 x kTileRows voxels)
+constexpr int kTileCols = 16;  // tile of the classify kernel: kTileCols (z) x kTileRows (y) voxels,
+constexpr int kTileRows = 8;   // one thread each
 
-// Launch geometry of the classify kernel: tiles of 32 (z) x kTileRows (y) voxels marching over
+// Launch geometry of the classify kernel: tiles of kTileCols (z) x kTileRows (y) voxels marching over
 // `xchunk` x-planes; enough x-chunks for several blocks per SM on small grids, long chunks (halo
 // reuse) on large ones.  slice = voxels one block can append to a bucket.
 inline void tiled_geometry(int nx, int ny, int nz, int* xchunk, int* gz, int* gy, int* gx)
 {
-    const int tzb = (nz + 31) / 32, tyb = (ny + kTileRows - 1) / kTileRows;
+    const int tzb = (nz + kTileCols - 1) / kTileCols, tyb = (ny + kTileRows - 1) / kTileRows;
     long long xc = (long long)nx * tzb * tyb / (148 * 8);
     xc = xc < 2 ? 2 : (xc > 32 ? 32 : xc);
     *xchunk = (int)xc;

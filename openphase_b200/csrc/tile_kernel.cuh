@@ -1,7 +1,7 @@
 // Tiled production path of the fused step: a classify kernel and one compute kernel per list length.
 //
 // classify (tile_classify_kernel)
-//   A block owns a (y, z) tile of TY x 32 voxels and marches along x over `xchunk` planes.  The 3x3x3
+//   A block owns a (y, z) tile of TY x kTileZ voxels and marches along x over `xchunk` planes.  The 3x3x3
 //   neighbourhoods come from a ring of three x-planes in shared memory (tile plus a one-voxel halo
 //   in y and z; periodic wrap by index arithmetic).  The grains present in the three planes of the
 //   window carry block-local slot numbers (at most kSlots, recycled as grains leave the window), and
@@ -26,28 +26,35 @@
 
 namespace opgpu {
 
-constexpr int kTileZ = 32;
-constexpr int kSlots = 16;           // distinct grains per 3-plane window
+constexpr int kTileZ = kTileCols;
+// distinct grains per 3-plane window: 16 for FP32 values, 14 for FP64 (its dense planes would
+// otherwise leave room for only two blocks per SM)
+template <class R>
+struct WindowSlots {
+    static constexpr int value = sizeof(R) == 8 ? 14 : 16;
+};
 constexpr int kSlotHash = 64;        // grain -> slot hash table entries
 constexpr int kTileVolSlots = 512;      // grain-volume hash of the compute kernels
 constexpr int kClassifyVolSlots = 256;  // grain-volume hash of the classify kernel (bulk voxels)
-constexpr int kTileTY = kTileRows;   // tile rows (blocks of 32 x kTileRows threads)
+constexpr int kTileTY = kTileRows;   // tile rows (blocks of kTileZ x kTileRows threads)
 
 template <int TY>
 struct TileGeom {
     static constexpr int kRows = TY + 2;
     static constexpr int kCols = kTileZ + 2;
     static constexpr int kRecs = kRows * kCols;
-    static constexpr int NT = 32 * TY;
+    static constexpr int NT = kTileZ * TY;
 };
 
 template <class R, int KS, int TY>
 struct TileSmem {
     using Geo = TileGeom<TY>;
+    static constexpr int kSlots = WindowSlots<R>::value;
     R dense[kSlots][3][Geo::kRecs];          // per-slot values of the three ring planes (zero where absent)
     double vol_sum[kClassifyVolSlots];
     uint64_t slotl[3][Geo::kRecs];           // slot ids of the record in entry order, 4 bits each
     uint32_t word[3][Geo::kRecs];            // slot bitmask of the record | (more than one field) << 31
+                                             // | (a grain of the record has no slot) << 30
     int vol_key[kClassifyVolSlots];
     int grain_of[kSlots];                    // slot -> grain (-1 = free)
     int lastpos[kSlots];                     // last window position where the slot's grain occurs
@@ -59,7 +66,6 @@ struct TileSmem {
     unsigned long long cnt[3];
     uint8_t hslot[kSlotHash];                // grain -> slot hash: slot
     uint8_t cntr[3][Geo::kRecs];             // entries per record
-    uint8_t bad[3];                          // ring plane holds a grain without slot
     uint8_t tomb;                            // deleted hash entries
 };
 
@@ -201,6 +207,7 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
     {
         const int g = S.pending[t];
         const bool valid = g >= 0;
+        constexpr int kSlots = WindowSlots<R>::value;
         const bool is_free = t < kSlots && (S.grain_of[t] < 0 || S.lastpos[t] < wpos - 2);
         const unsigned fm = __ballot_sync(0xffffffffu, is_free);
         const unsigned vm = __ballot_sync(0xffffffffu, valid);
@@ -224,7 +231,7 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         }
         if (t == 0)
         {
-            S.bad[rs] = fb ? 1 : 0;
+            (void)fb;   // grains left without a slot are marked per record in step 3
             if (S.tomb > 24)
             {
                 for (int h = 0; h < kSlotHash; h++) S.hkey[h] = -1;
@@ -245,6 +252,7 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         for (uint32_t m = S.word[rs][r] & 0xFFFFu; m; m &= m - 1u) S.dense[__ffs(m) - 1][rs][r] = R(0);
         uint32_t msk = 0;
         uint64_t lst = 0;
+        bool unslotted = false;
         const int c = cr[i];
         for (int s = 0; s < c; s++)
         {
@@ -255,13 +263,13 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
                 if (q == s) { g = gr[i][q]; val = vr[i][q]; }
             if (s >= PR::kKeep) { g = a.idx_in[s * N + vv[i]]; val = vin[s * N + vv[i]]; }
             const int k = find_slot(S.hkey, S.hslot, g);
-            if (k < 0) { S.bad[rs] = 1; continue; }
+            if (k < 0) { unslotted = true; continue; }
             S.dense[k][rs][r] = val;
             lst |= (uint64_t)k << (4 * s);
             msk |= 1u << k;
             S.lastpos[k] = wpos;
         }
-        S.word[rs][r] = msk | (c > 1 ? 0x80000000u : 0u);
+        S.word[rs][r] = msk | (c > 1 ? 0x80000000u : 0u) | (unslotted ? 0x40000000u : 0u);
         S.slotl[rs][r] = lst;
         S.cntr[rs][r] = (uint8_t)c;
     }
@@ -297,7 +305,7 @@ __device__ __forceinline__ void append_fresh(const TileSmem<R, KS, TY>& S, int p
 }
 
 template <class R, int KS, int TY, int NS>
-__global__ void __launch_bounds__(32 * TY)
+__global__ void __launch_bounds__(kTileZ * TY)
 tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, int xchunk)
 {
     using Geo = TileGeom<TY>;
@@ -307,7 +315,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
 
-    const int tz = threadIdx.x, ty = threadIdx.y, t = ty * 32 + tz;
+    const int tz = threadIdx.x, ty = threadIdx.y, t = ty * kTileZ + tz;
     const int z0 = blockIdx.x * kTileZ, y0 = blockIdx.y * TY, x0 = blockIdx.z * xchunk;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int x1 = min(x0 + xchunk, nx);
@@ -322,6 +330,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     R* __restrict__ vout = static_cast<R*>(a.val_out);
 
     for (int i = t; i < kClassifyVolSlots; i += NT) { S.vol_key[i] = -1; S.vol_sum[i] = 0.0; }
+    constexpr int kSlots = WindowSlots<R>::value;
     for (int i = t; i < kSlots * 3 * Geo::kRecs; i += NT) (&S.dense[0][0][0])[i] = R(0);
     for (int i = t; i < 3 * Geo::kRecs; i += NT) (&S.word[0][0])[i] = 0u;
     if (t < kSlots) { S.grain_of[t] = -1; S.lastpos[t] = -1000; }
@@ -351,18 +360,11 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         if (j < 2 || !inside) continue;
         const int x = x0 + j - 2;
         const int sl0 = (j - 2) % 3, sl1 = (j - 1) % 3, sl2 = j % 3;
-        const bool window_bad = S.bad[0] | S.bad[1] | S.bad[2];
         const long long v = (long long)x * plane + (long long)y * nz + z;
 
         const int c = S.cntr[sl1][rec0];
         ein += c;
-        // ---- flag and (27-point stencils) candidate discovery in one pass over the neighbours ----
-        uint64_t ls = 0;
-        int n = c;
-        bool over = window_bad || c > kListCap;
-        if (!over) ls = S.slotl[sl1][rec0];   // c <= kListCap entries, unused nibbles are zero
-        const uint32_t own = S.word[sl1][rec0] & 0xFFFFu;
-        uint32_t seen = own;
+        // ---- flag and (27-point stencils) candidate discovery over the neighbours ----------------
         uint32_t multi = 0;
 #pragma unroll
         for (int q = 0; q < 27; q++)
@@ -371,6 +373,14 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
             const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
             multi |= S.word[pl][r];
         }
+        // a neighbour holding a grain the window has no slot for: the general path
+        const bool window_bad = (multi >> 30) & 1u;
+        uint64_t ls = 0;
+        int n = c;
+        bool over = window_bad || c > kListCap;
+        if (!over) ls = S.slotl[sl1][rec0];   // c <= kListCap entries, unused nibbles are zero
+        const uint32_t own = S.word[sl1][rec0] & 0xFFFFu;
+        uint32_t seen = own;
         // candidates in the reference's order: new grains of each neighbour in stencil order and
         // neighbour-list order (a rolled loop, entered only when some neighbour holds a new grain)
         if (NS == 27 && !over && ((multi & 0xFFFFu) & ~own))
@@ -786,7 +796,7 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     if (e != cudaSuccess) return (int)e;
     e = cudaMemsetAsync(a.slow2_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return (int)e;
-    kern<<<dim3(gz, gy, gx), dim3(32, kTileTY), smem, s>>>(p, a, xchunk);
+    kern<<<dim3(gz, gy, gx), dim3(kTileZ, kTileTY), smem, s>>>(p, a, xchunk);
     if (info && info->after_classify)
     {
         e = cudaEventRecord(static_cast<cudaEvent_t>(info->after_classify), s);
