@@ -341,6 +341,8 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     if (t == 0) { S.woff = 0u; S.crowded = 0u; S.tomb = 0; }
     unsigned wide = 0, ein = 0, eout = 0;
     uint32_t st = 0;
+    int acc_g = -1;        // bulk-voxel volume accumulator of this thread
+    double acc_v = 0.0;
     int cr[PlaneRegs<TY>::kPer];
     prefetch_counts<TY>(p, a, x0 == 0 ? nx - 1 : x0 - 1, y0, z0, t, cr);
     __syncthreads();
@@ -412,7 +414,18 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
                 const R phi = static_cast<const R*>(a.val_in)[s * N + v];
                 a.idx_out[s * N + v] = (int16_t)g;
                 vout[s * N + v] = phi;
-                if (in_volume_window(p, v)) vol_insert_n(S.vol_key, S.vol_sum, kClassifyVolSlots, a.vol_acc, g, (double)phi);
+                if (in_volume_window(p, v))
+                {
+                    // consecutive bulk voxels of a thread mostly belong to one grain: sum them in a
+                    // register before the shared-memory add
+                    if (g != acc_g)
+                    {
+                        if (acc_g >= 0) vol_insert_n(S.vol_key, S.vol_sum, kClassifyVolSlots, a.vol_acc, acc_g, acc_v);
+                        acc_g = g;
+                        acc_v = 0.0;
+                    }
+                    acc_v += (double)phi;
+                }
             }
             eout += c;
             continue;
@@ -469,6 +482,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     __syncthreads();
     if (t >= 2 && t <= kListCap) a.bucket_count[t * nblocks + blin] = S.nb[t];
     if (t == 0 && S.crowded) atomicAdd(&a.counters[kCntCrowdedLast], (unsigned long long)S.crowded);
+    if (acc_g >= 0) vol_insert_n(S.vol_key, S.vol_sum, kClassifyVolSlots, a.vol_acc, acc_g, acc_v);
     flush_block(a, wide, ein, eout, st, S.cnt, S.vol_key, S.vol_sum, kClassifyVolSlots, t, NT);
 }
 
@@ -494,8 +508,16 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     R* __restrict__ vout = static_cast<R*>(a.val_out);
     uint32_t st = 0;
     unsigned eout = 0;
-    for (unsigned e = t; e < cnt; e += blockDim.x)
+    const unsigned lane = t & 31u;
+    for (unsigned base = t - lane; base < cnt; base += blockDim.x)   // the same trip count per warp
     {
+        const unsigned e = base + lane;
+        int vg[N];       // the voxel's contributions to the grain volumes (grain -1: none)
+        double vw[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) { vg[i] = -1; vw[i] = 0.0; }
+        if (e < cnt)
+        {
         const int2 ent = list[e];
         const long long v = ent.x & 0x7fffffff;
         const int flag = (ent.x >> 31) ? 2 : 1;
@@ -735,7 +757,7 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
                 if (!isfinite((double)w)) st |= kStNonFinite;
                 a.idx_out[pos * N_ + v] = (int16_t)g[i];
                 vout[pos * N_ + v] = w;
-                if (in_volume_window(p, v)) vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, g[i], (double)w);
+                if (in_volume_window(p, v)) { vg[i] = g[i]; vw[i] = (double)w; }
                 pos++;
             }
         }
@@ -743,6 +765,19 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
         if (m > KS) st |= kStOverflowK;
         a.cnt_out[v] = (uint8_t)pos;
         eout += pos;
+        }
+        // one shared-memory add per grain and warp: the lanes adding to the same grain sum first
+#pragma unroll
+        for (int i = 0; i < N; i++)
+        {
+            const unsigned peers = __match_any_sync(0xffffffffu, vg[i]);
+            if (vg[i] >= 0)
+            {
+                double s = 0.0;
+                for (unsigned mk = peers; mk; mk &= mk - 1u) s += __shfl_sync(peers, vw[i], __ffs(mk) - 1);
+                if (lane == (unsigned)(__ffs(peers) - 1)) vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, vg[i], s);
+            }
+        }
     }
     flush_block(a, 0u, 0u, eout, st, s_cnt, s_key, s_sum, kTileVolSlots, t, blockDim.x);
 }
