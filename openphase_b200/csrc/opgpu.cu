@@ -64,8 +64,6 @@ struct opgpu_ctx {
     unsigned long long* d_counters = nullptr;
     int* d_slow_list = nullptr;      // overflow worklist of the tiled kernel (capacity N)
     unsigned* d_slow_count = nullptr;
-    int* d_slow2_list = nullptr;     // second general-path worklist (long lists)
-    unsigned* d_slow2_count = nullptr;
     // work buffer of the classify / compute split (see tile_kernel.cuh)
     unsigned char* d_wl = nullptr;
     long long wl_slice = 0;
@@ -444,8 +442,6 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
     }
     if (dalloc(&ctx->d_slow_list, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
     if (dalloc(&ctx->d_slow_count, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
-    if (dalloc(&ctx->d_slow2_list, (size_t)ctx->n) != cudaSuccess) return bail(OPGPU_E_CUDA);
-    if (dalloc(&ctx->d_slow2_count, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
     {
         int xchunk = 0, gz = 0, gy = 0, gx = 0;
         tiled_geometry(g.nx, g.ny, g.nz, &xchunk, &gz, &gy, &gx);
@@ -490,8 +486,6 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     dfree(ctx->d_slow_list);
     dfree(ctx->d_slow_count);
-    dfree(ctx->d_slow2_list);
-    dfree(ctx->d_slow2_count);
     dfree(ctx->d_wl);
     dfree(ctx->d_bucket); dfree(ctx->d_bucket_count);
     dfree(ctx->d_status);
@@ -795,7 +789,6 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
         a.grot = ctx->d_grot;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
-        a.slow2_list = ctx->d_slow2_list; a.slow2_count = ctx->d_slow2_count;
         a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
         a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
         a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;

@@ -113,8 +113,6 @@ struct StepArrays {
     int* slow_list;            // [slow_cap]
     unsigned* slow_count;      // reset by the launcher before every step
     unsigned slow_cap;
-    int* slow2_list;           // [slow_cap] lists longer than the first general-path pass holds
-    unsigned* slow2_count;
     // work buffer between the classify kernel and the per-length compute kernels: every list is a
     // record of n fields (int16 grains padded to 8 bytes, then n values, then n Laplacians) packed
     // in its classify block's byte slice; bucket entries (voxel | flag2 << 31, record offset)

@@ -558,14 +558,11 @@ __device__ __forceinline__ int gather_list(const StepParams& p, const uint8_t* _
 // working arrays in local memory (capacity KL fields).  This is the general path: the full-grid
 // kernel below and the overflow kernel of the tiled step (lists longer than the tiled kernel's
 // capacity) both run it.
-// ANISO: gradients for anisotropic energies.  With `defer` (a worklist with its counter and
-// capacity), a voxel whose list exceeds KL is appended there, untouched, for a larger-capacity pass.
+// ANISO: gradients for anisotropic energies.
 template <class R, int KS, int KL, bool ANISO>
 __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const StepArrays& a, long long v,
                                                    int* s_key, double* s_sum, int nslots, unsigned& wide,
-                                                   unsigned& ein, unsigned& eout, uint32_t& st, bool count_in,
-                                                   int* defer = nullptr, unsigned* defer_count = nullptr,
-                                                   unsigned defer_cap = 0)
+                                                   unsigned& ein, unsigned& eout, uint32_t& st, bool count_in)
 {
     const long long N = p.n;
     const uint8_t* __restrict__ cnt = a.cnt_in;
@@ -600,17 +597,7 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     R val[KL], lap[KL], sg[KP];
     double pv[KP], pos[KL], neg[KL];
     R grad[ANISO ? 3 * KL : 1];
-    uint32_t st_list = 0;
-    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, ANISO ? grad : nullptr, st_list);
-    if ((st_list & kStOverflowList) && defer)
-    {
-        const unsigned slot = atomicAdd(defer_count, 1u);
-        if (slot < defer_cap) defer[slot] = (int)v;
-        else st |= kStOverflowList;
-        wide = 0;
-        return;
-    }
-    st |= st_list;
+    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, ANISO ? grad : nullptr, st);
     const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1, ANISO ? grad : nullptr};
     int m = list_step<R>(p, a, sc, n, flag, st);
     if (m > KS) { st |= kStOverflowK; m = KS; }

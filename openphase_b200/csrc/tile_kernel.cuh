@@ -19,10 +19,11 @@
 //   One kernel per list length N = 2..kListCap, each CUDA block draining one classify block's
 //   slice: fully unrolled, register-only pair kinetics, driving force, projection, merge and
 //   finalize (the operation order of list_step), new record written to the output state.
-// Lists longer than kListCap and windows with more than kSlots distinct grains go to the overflow
-// worklist, processed by the general per-voxel kernel.
+// Lists longer than kListCap and voxels next to a grain without a window slot go to the general-path
+// worklist, processed one warp per voxel (warp_step.cuh).
 #pragma once
 #include "step_kernel.cuh"
+#include "warp_step.cuh"
 
 namespace opgpu {
 
@@ -782,39 +783,6 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     flush_block(a, 0u, 0u, eout, st, s_cnt, s_key, s_sum, kTileVolSlots, t, blockDim.x);
 }
 
-// Voxels whose field + candidate list exceeds the split kernels' capacity, through the general
-// per-voxel path (grid-stride over the worklist; the classify kernel already counted them as wide
-// and counted their input entries).
-// TIER 1 takes the classify kernel's worklist with a list capacity of KL and defers longer lists to
-// the second worklist; TIER 2 takes that one with the large capacity.
-template <class R, int KS, int KL, int TIER>
-__global__ void __launch_bounds__(128) overflow_step_kernel(const __grid_constant__ StepParams p, const StepArrays a)
-{
-    __shared__ int s_key[kVolSlots];
-    __shared__ double s_sum[kVolSlots];
-    __shared__ unsigned long long s_cnt[3];
-    for (int i = threadIdx.x; i < kVolSlots; i += blockDim.x) { s_key[i] = -1; s_sum[i] = 0.0; }
-    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0ull;
-    __syncthreads();
-    const int* list = TIER == 1 ? a.slow_list : a.slow2_list;
-    const unsigned total = min(TIER == 1 ? *a.slow_count : *a.slow2_count, a.slow_cap);
-    if (TIER == 1 && blockIdx.x == 0 && threadIdx.x == 0)
-        atomicAdd(&a.counters[kCntGeneralLast], (unsigned long long)total);
-    uint32_t st = 0;
-    unsigned eo_sum = 0;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
-    {
-        unsigned wide = 0, ein = 0, eout = 0;
-        if (TIER == 1)
-            voxel_step_generic<R, KS, KL, false>(p, a, list[i], s_key, s_sum, kVolSlots, wide, ein, eout, st, false,
-                                                 a.slow2_list, a.slow2_count, a.slow_cap);
-        else
-            voxel_step_generic<R, KS, KL, false>(p, a, list[i], s_key, s_sum, kVolSlots, wide, ein, eout, st, false);
-        eo_sum += eout;
-    }
-    flush_block(a, 0u, 0u, eo_sum, st, s_cnt, s_key, s_sum, kVolSlots, threadIdx.x, blockDim.x);
-}
-
 template <class R, int KS, int KL, int NS>
 int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, LaunchInfo* info)
 {
@@ -829,8 +797,6 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     if (e != cudaSuccess) return (int)e;
     e = cudaMemsetAsync(a.slow_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return (int)e;
-    e = cudaMemsetAsync(a.slow2_count, 0, sizeof(unsigned), s);
-    if (e != cudaSuccess) return (int)e;
     kern<<<dim3(gz, gy, gx), dim3(kTileZ, kTileTY), smem, s>>>(p, a, xchunk);
     if (info && info->after_classify)
     {
@@ -844,11 +810,15 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     list_compute_kernel<R, 6, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 7, KS><<<nblocks, 128, 0, s>>>(p, a);
     list_compute_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a);
-    // general path: lists up to 12 fields with four warps per SM, then the longer ones with one
-    // warp per SM (the per-thread working arrays then stay in L1)
-    overflow_step_kernel<R, KS, 12, 1><<<148, 128, 0, s>>>(p, a);
-    overflow_step_kernel<R, KS, KL, 2><<<148, 32, 0, s>>>(p, a);
-    if (info) info->kernels += 10;
+    // general path: one warp per voxel of the worklist
+    {
+        auto gk = warp_general_kernel<R, KS, KL>;
+        const size_t wsm = 4 * sizeof(WarpScratch<R, KL>);
+        e = cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+        if (e != cudaSuccess) return (int)e;
+        gk<<<148 * 4, 128, wsm, s>>>(p, a);
+    }
+    if (info) info->kernels += 9;
     return (int)cudaGetLastError();
 }
 
