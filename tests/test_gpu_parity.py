@@ -192,3 +192,32 @@ def test_overflow_is_reported_not_silent():
     st = ctx.step(case.dt, 5)
     assert st & 0b11
     assert ctx.stats()["overflow_voxels"] > 0
+
+
+def test_single_grain_and_tiny_grids_are_stable():
+    """Edge cases: a grid holding one grain is bulk everywhere (the step is the identity), and grids
+    thinner than a classify tile in every direction step like the generic kernel."""
+    one = Case(20, 12, 9, 1, seed=1, iwidth=4.0, dt=0.1, name="one_grain")
+    ctx = Context.from_case(one, precision="fp64", k_slots=8)
+    before = ctx.download()
+    assert ctx.step(one.dt, 3) == 0
+    after = ctx.download()
+    assert all(np.array_equal(x, y) for x, y in zip(before, after))
+    assert ctx.stats()["wide_last"] == 0
+    assert abs(ctx.grains()["volume"][0] - one.n) <= 1e-9
+    tiny = Case(6, 5, 7, 4, seed=2, iwidth=3.0, dt=0.1, name="tiny")
+    state = tiny.initial_state()
+    a = Context.from_case(tiny, precision="fp64", k_slots=16, state=state)
+    b = Context.from_case(tiny, precision="fp64", k_slots=16, state=state)
+    b.set_kernel_variant("generic")
+    ora = Oracle(tiny, *state)
+    for _ in range(3):
+        a.step(tiny.dt, 5)
+        b.step(tiny.dt, 5)
+        ora.step(5)
+        ca, ia, va = a.download()
+        cb, ib, vb = b.download()
+        assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
+        assert np.max(np.abs(va - vb)) <= 1e-12
+        r = compare_states((ca, ia, va), ora.state(positive_only=True), tiny.ngrains)
+        assert r["non_borderline_mismatch_voxels"] == 0 and r["max_dphi"] <= 1e-9, r
