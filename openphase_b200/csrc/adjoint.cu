@@ -506,36 +506,26 @@ __device__ void limiter_iteration_reverse(int n, const double* val, double dt, c
         }
 }
 
-template <class R, int KS>
-__global__ void __launch_bounds__(64) adjoint_local_kernel(const __grid_constant__ StepParams p, const StepArrays a,
-                                                            const AdjArrays aa)
+// The adjoint of one wide voxel's step, from its list (own fields first, then candidates) with the
+// values and Laplacians the step used.  KL: capacity of the working arrays (the list-length
+// kernels pass their exact length, so that every loop has a fixed trip count).
+template <int KL, int KS>
+__device__ __forceinline__ void adjoint_core(const StepParams& p, const StepArrays& a, const AdjArrays& aa,
+                                             long long v, int flag, int n, int c, const int16_t* g0,
+                                             const double* val_in, const double* lap_in, uint32_t st)
 {
-    constexpr int KL = KAdjList;
-    constexpr int KP = KAdjPairs;
+    constexpr int KP = KL * (KL - 1) / 2;
     const long long N = p.n;
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= N) return;
-    const uint8_t* cnt = a.cnt_in;
-    const int16_t* gin = a.idx_in;
-    const R* vin = static_cast<const R*>(a.val_in);
-    const Neighbourhood nb(p, v);
-    const int c = cnt[v];
-    const int flag = voxel_flag(cnt, nb, v);
-    uint32_t st = 0;
-    if (flag == 0)
-    {
-        // bulk voxel: identity
-        for (int s = 0; s < c; s++) aa.lam_local[s * N + v] = aa.lam1[s * N + v];
-        aa.lcnt[v] = 0;
-        return;
-    }
     int16_t g[KL];
-    R vr[KL], lr[KL];
-    const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, g, vr, lr, nullptr, st);
     double val[KL], lap[KL], lval[KL], llap[KL];
-    for (int k = 0; k < n; k++) { val[k] = (double)vr[k]; lap[k] = (double)lr[k]; lval[k] = 0.0; llap[k] = 0.0; }
-    int16_t g0[KL];
-    for (int k = 0; k < n; k++) g0[k] = g[k];
+    for (int k = 0; k < n; k++)
+    {
+        g[k] = g0[k];
+        val[k] = val_in[k];
+        lap[k] = lap_in[k];
+        lval[k] = 0.0;
+        llap[k] = 0.0;
+    }
     const int G = p.ngrains;
     const int np = n * (n - 1) / 2;
     const double dt = p.dt;
@@ -846,6 +836,80 @@ __global__ void __launch_bounds__(64) adjoint_local_kernel(const __grid_constant
     if (st) atomicOr(a.status, st);
 }
 
+
+// Bulk voxels of the state before the step are carried over unchanged: identity adjoint.  (The
+// wide voxels are left to the list-length kernels and the worklist kernel.)
+__global__ void adjoint_bulk_kernel(const __grid_constant__ StepParams p, const uint8_t* __restrict__ cnt,
+                                    const AdjArrays aa)
+{
+    const long long N = p.n;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const Neighbourhood nb(p, v);
+    if (voxel_flag(cnt, nb, v) != 0) return;
+    const int c = cnt[v];
+    for (int s = 0; s < c; s++) aa.lam_local[s * N + v] = aa.lam1[s * N + v];
+    aa.lcnt[v] = 0;
+}
+
+// Wide voxels whose list has N fields, from the classify kernel's work records (the lists, values
+// and Laplacians the forward step used; own fields are the leading nonzero values).
+template <class R, int N, int KS>
+__global__ void __launch_bounds__(128) adjoint_list_kernel(const __grid_constant__ StepParams p, const StepArrays a,
+                                                            const AdjArrays aa)
+{
+    const unsigned cnt = a.bucket_count[N * (long long)gridDim.x + blockIdx.x];
+    const int2* __restrict__ list = a.bucket + (long long)N * a.bucket_cap + (long long)blockIdx.x * a.slice;
+    const unsigned char* __restrict__ wbase = a.wl + (long long)blockIdx.x * a.wl_slice;
+    constexpr int kPad = ((2 * N + 7) / 8) * 8;
+    for (unsigned e = threadIdx.x; e < cnt; e += blockDim.x)
+    {
+        const int2 ent = list[e];
+        const long long v = ent.x & 0x7fffffff;
+        const int flag = (ent.x >> 31) ? 2 : 1;
+        const int16_t* __restrict__ rg = reinterpret_cast<const int16_t*>(wbase + ent.y);
+        const R* __restrict__ rv = reinterpret_cast<const R*>(wbase + ent.y + kPad);
+        int16_t g[N];
+        double val[N], lap[N];
+        int c = 0;
+        bool own = true;
+#pragma unroll
+        for (int k = 0; k < N; k++)
+        {
+            g[k] = rg[k];
+            val[k] = (double)rv[k];
+            lap[k] = (double)rv[N + k];
+            own = own && val[k] != 0.0;
+            c += own ? 1 : 0;
+        }
+        adjoint_core<N, KS>(p, a, aa, v, flag, N, c, g, val, lap, 0u);
+    }
+}
+
+// Wide voxels of the classify kernel's general-path worklist: the general gather, then the core.
+template <class R, int KS>
+__global__ void __launch_bounds__(64) adjoint_worklist_kernel(const __grid_constant__ StepParams p, const StepArrays a,
+                                                               const AdjArrays aa)
+{
+    constexpr int KL = KAdjList;
+    const unsigned total = min(*a.slow_count, a.slow_cap);
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+    {
+        const long long v = a.slow_list[i];
+        const Neighbourhood nb(p, v);
+        const int c = a.cnt_in[v];
+        const int flag = voxel_flag(a.cnt_in, nb, v);
+        uint32_t st = 0;
+        int16_t g[KL];
+        R vr[KL], lr[KL];
+        const int n = gather_list<R, KL>(p, a.cnt_in, a.idx_in, static_cast<const R*>(a.val_in), nb, v, g, vr, lr,
+                                         nullptr, st);
+        double val[KL], lap[KL];
+        for (int k = 0; k < n; k++) { val[k] = (double)vr[k]; lap[k] = (double)lr[k]; }
+        adjoint_core<KL, KS>(p, a, aa, v, flag, n, c, g, val, lap, st);
+    }
+}
+
 // lambda_t(u, s) = own part + sum_q w_q * (adjoint of the Laplacian of grain g_s at u - d_q)
 __global__ void adjoint_gather_kernel(const __grid_constant__ StepParams p, const uint8_t* __restrict__ cnt,
                                       const int16_t* __restrict__ idx, const AdjArrays aa, double* __restrict__ lam0)
@@ -894,30 +958,33 @@ int launch_tlm_step(const StepParams& p, const StepArrays& a, const AdjArrays& a
     return (int)cudaGetLastError();
 }
 
+template <class R, int KS>
+static void adjoint_kernels(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int nblocks, cudaStream_t s)
+{
+    adjoint_list_kernel<R, 2, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 3, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 4, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 5, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 6, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 7, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_worklist_kernel<R, KS><<<148 * 4, 64, 0, s>>>(p, a, aa);
+}
+
 int launch_adjoint_step(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int k_slots, bool fp32,
-                        double* lam0, void* stream)
+                        int nblocks, double* lam0, void* stream)
 {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const unsigned gb = grid_of(p.n, 64);
-    if (fp32)
+    adjoint_bulk_kernel<<<grid_of(p.n, 256), 256, 0, s>>>(p, a.cnt_in, aa);
+    switch (k_slots * 2 + (fp32 ? 1 : 0))
     {
-        switch (k_slots)
-        {
-            case 8:  adjoint_local_kernel<float, 8><<<gb, 64, 0, s>>>(p, a, aa); break;
-            case 12: adjoint_local_kernel<float, 12><<<gb, 64, 0, s>>>(p, a, aa); break;
-            case 16: adjoint_local_kernel<float, 16><<<gb, 64, 0, s>>>(p, a, aa); break;
-            default: return -1;
-        }
-    }
-    else
-    {
-        switch (k_slots)
-        {
-            case 8:  adjoint_local_kernel<double, 8><<<gb, 64, 0, s>>>(p, a, aa); break;
-            case 12: adjoint_local_kernel<double, 12><<<gb, 64, 0, s>>>(p, a, aa); break;
-            case 16: adjoint_local_kernel<double, 16><<<gb, 64, 0, s>>>(p, a, aa); break;
-            default: return -1;
-        }
+        case 16: adjoint_kernels<double, 8>(p, a, aa, nblocks, s); break;
+        case 17: adjoint_kernels<float, 8>(p, a, aa, nblocks, s); break;
+        case 24: adjoint_kernels<double, 12>(p, a, aa, nblocks, s); break;
+        case 25: adjoint_kernels<float, 12>(p, a, aa, nblocks, s); break;
+        case 32: adjoint_kernels<double, 16>(p, a, aa, nblocks, s); break;
+        case 33: adjoint_kernels<float, 16>(p, a, aa, nblocks, s); break;
+        default: return -1;
     }
     adjoint_gather_kernel<<<grid_of(p.n, 128), 128, 0, s>>>(p, a.cnt_in, a.idx_in, aa, lam0);
     return (int)cudaGetLastError();

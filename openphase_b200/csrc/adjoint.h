@@ -33,10 +33,11 @@ struct AdjArrays {
 // One FP64 step with tangents (writes the new state like the step kernels, and its tangent).
 int launch_tlm_step(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int k_slots, void* stream);
 // Adjoint of one step: a.cnt_in/idx_in/val_in hold the state before the step, aa the state after it
-// and its adjoint; writes the adjoint of the state before the step to lam0 and accumulates the
-// parameter gradients.
+// and its adjoint; the classify kernel has just run on the state before the step (its work
+// records, buckets and worklist in a; nblocks its block count).  Writes the adjoint of the state
+// before the step to lam0 and accumulates the parameter gradients.
 int launch_adjoint_step(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int k_slots, bool fp32,
-                        double* lam0, void* stream);
+                        int nblocks, double* lam0, void* stream);
 // lam[s][v] = dLdV[idx[s][v]] on the stored entries (adjoint of a loss on the grain volumes).
 int launch_lambda_init(long long n, const uint8_t* cnt, const int16_t* idx, const double* dLdV, double* lam,
                        void* stream);

@@ -1241,9 +1241,21 @@ extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
     aa.lam_local = ctx->d_lam_local; aa.lcnt = ctx->d_lcnt; aa.lidx = ctx->d_lidx; aa.llam = ctx->d_llam;
     aa.gsig = ctx->d_gsig; aa.gmu = ctx->d_gmu; aa.gdg = ctx->d_gdg;
     double* lam0 = ctx->d_lam[1 - ctx->lam_cur];   // every stored entry of the slot's state is written
-    if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, lam0, ctx->stream))
+    // the forward's lists of the slot's state: the classify kernel (its bulk copies go to the spare
+    // state buffer, its volume sums and counters are discarded)
+    a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
+    a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
+    a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
+    a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;
+    const int nblocks = ctx->fp32 ? launch_classify_f32(sp, a, ctx->K, ctx->stream)
+                                  : launch_classify_f64(sp, a, ctx->K, ctx->stream);
+    if (nblocks < 0) return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: classify launch");
+    CK(cudaMemsetAsync(ctx->d_vol_acc, 0, (size_t)ctx->G * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_counters, 0, 3 * sizeof(unsigned long long), ctx->stream));   // wide, entries in/out
+    CK(cudaMemsetAsync(ctx->d_counters + kCntCrowdedLast, 0, sizeof(unsigned long long), ctx->stream));
+    if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, nblocks, lam0, ctx->stream))
         return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: launch");
-    ctx->kernel_launches += 2;
+    ctx->kernel_launches += 11;
     ctx->lam_cur = 1 - ctx->lam_cur;
     // the state before the step becomes the current state (the adjoint is aligned with it)
     if (uint32_t r = copy_state(ctx, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur], s.cnt, s.idx, s.val)) return r;

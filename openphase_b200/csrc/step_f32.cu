@@ -8,4 +8,9 @@ int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int v
 {
     return launch_step<float>(p, a, k_slots, variant, stream, info);
 }
+
+int launch_classify_f32(const StepParams& p, const StepArrays& a, int k_slots, void* stream)
+{
+    return launch_classify<float>(p, a, k_slots, stream);
+}
 }  // namespace opgpu

@@ -10,6 +10,11 @@ int launch_step_f64(const StepParams& p, const StepArrays& a, int k_slots, int v
     return launch_step<double>(p, a, k_slots, variant, stream, info);
 }
 
+int launch_classify_f64(const StepParams& p, const StepArrays& a, int k_slots, void* stream)
+{
+    return launch_classify<double>(p, a, k_slots, stream);
+}
+
 __global__ void dg_pair_kernel(const __grid_constant__ StepParams p, const double* __restrict__ dg,
                                const int16_t* __restrict__ gphase, double* __restrict__ out)
 {

@@ -822,6 +822,40 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     return (int)cudaGetLastError();
 }
 
+// The classify kernel alone (work records, length buckets, general-path worklist, bulk copies):
+// the adjoint reverses the lists it leaves.  Returns the number of classify blocks (the slices of
+// the buckets) or a negative error.
+template <class R, int KS, int NS>
+int launch_classify_ns(const StepParams& p, const StepArrays& a, void* stream)
+{
+    using Smem = TileSmem<R, KS, kTileTY>;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int xchunk = 0, gz = 0, gy = 0, gx = 0;
+    tiled_geometry(p.nx, p.ny, p.nz, &xchunk, &gz, &gy, &gx);
+    auto kern = tile_classify_kernel<R, KS, kTileTY, NS>;
+    const size_t smem = sizeof(Smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return -(int)e;
+    e = cudaMemsetAsync(a.slow_count, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return -(int)e;
+    kern<<<dim3(gz, gy, gx), dim3(kTileZ, kTileTY), smem, s>>>(p, a, xchunk);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? gz * gy * gx : -(int)e;
+}
+
+template <class R>
+int launch_classify(const StepParams& p, const StepArrays& a, int k_slots, void* stream)
+{
+    const bool ns27 = p.ns == 27;
+    switch (k_slots)
+    {
+        case 8:  return ns27 ? launch_classify_ns<R, 8, 27>(p, a, stream) : launch_classify_ns<R, 8, 7>(p, a, stream);
+        case 12: return ns27 ? launch_classify_ns<R, 12, 27>(p, a, stream) : launch_classify_ns<R, 12, 7>(p, a, stream);
+        case 16: return ns27 ? launch_classify_ns<R, 16, 27>(p, a, stream) : launch_classify_ns<R, 16, 7>(p, a, stream);
+        default: return -1;
+    }
+}
+
 template <class R, int KS, int KL>
 int launch_tiled(const StepParams& p, const StepArrays& a, void* stream, LaunchInfo* info)
 {
