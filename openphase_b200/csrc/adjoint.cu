@@ -13,9 +13,13 @@
 //
 // Kernels
 //   tlm_step_kernel      one forward step of the FP64 form with dual numbers: new state + tangent
-//   adjoint_local_kernel per voxel: recompute the step's arithmetic (same operation order as the
-//                        forward), reverse it: adjoint of the voxel's own input values, of the
-//                        Laplacians of its list, and the parameter gradients
+//   adjoint_core         per wide voxel: recompute the step's arithmetic (same operation order as
+//                        the forward), reverse it: adjoint of the voxel's own input values, of the
+//                        Laplacians of its list, and the parameter gradients; driven by
+//   adjoint_list_kernel  the classify kernel's work records of one list length (the forward's own
+//                        lists, values and Laplacians), and by
+//   adjoint_worklist_kernel the voxels of the general-path worklist (general gather);
+//   adjoint_bulk_kernel  bulk voxels: the adjoint passes through
 //   adjoint_gather_kernel adjoint of the stored values at t: own part plus the transposed stencil
 //                        over the neighbours' Laplacian adjoints
 // Compiled with --fmad=false so that the recomputed FP64 arithmetic repeats the forward's.
