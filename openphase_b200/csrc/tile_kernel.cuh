@@ -368,13 +368,22 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         const int c = S.cntr[sl1][rec0];
         ein += c;
         // ---- flag and (27-point stencils) candidate discovery over the neighbours ----------------
-        uint32_t multi = 0;
-#pragma unroll
-        for (int q = 0; q < 27; q++)
+        // One unrolled pass over the 27 bitmask words: the flag bits, and the stencil positions
+        // whose record holds a grain not seen at an earlier position (nor in the voxel itself).
+        const uint32_t own = S.word[sl1][rec0] & 0xFFFFu;
+        uint32_t multi = 0, qfresh = 0;
         {
-            const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
-            const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
-            multi |= S.word[pl][r];
+            uint32_t seen = own;
+#pragma unroll
+            for (int q = 0; q < 27; q++)
+            {
+                const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
+                const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
+                const uint32_t w = S.word[pl][r];
+                multi |= w;
+                if (w & 0xFFFFu & ~seen) qfresh |= 1u << q;
+                seen |= w;
+            }
         }
         // a neighbour holding a grain the window has no slot for: the general path
         const bool window_bad = (multi >> 30) & 1u;
@@ -382,25 +391,20 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         int n = c;
         bool over = window_bad || c > kListCap;
         if (!over) ls = S.slotl[sl1][rec0];   // c <= kListCap entries, unused nibbles are zero
-        const uint32_t own = S.word[sl1][rec0] & 0xFFFFu;
-        uint32_t seen = own;
         // candidates in the reference's order: new grains of each neighbour in stencil order and
-        // neighbour-list order (a rolled loop, entered only when some neighbour holds a new grain)
-        if (NS == 27 && !over && ((multi & 0xFFFFu) & ~own))
+        // neighbour-list order.  Only the positions marked above bring new grains; the words of the
+        // others add nothing to `seen`, so visiting the marked ones in order gives the same list.
+        if (NS == 27 && !over && qfresh)
         {
-#pragma unroll 1
-            for (int q = 0; q < 27; q++)
+            uint32_t seen = own;
+            for (uint32_t m = qfresh; m; m &= m - 1u)
             {
-                if (q == 13) continue;
+                const int q = __ffs(m) - 1;
                 const int pl = q < 9 ? sl0 : (q < 18 ? sl1 : sl2);
                 const int r = rec0 + ((q / 3) % 3 - 1) * kC + (q % 3 - 1);
                 const uint32_t w = S.word[pl][r] & 0xFFFFu;
-                const uint32_t fresh = w & ~seen;
-                if (fresh)
-                {
-                    append_fresh(S, pl, r, fresh, ls, n, over);
-                    if (over) break;
-                }
+                append_fresh(S, pl, r, w & ~seen, ls, n, over);
+                if (over) break;
                 seen |= w;
             }
         }
@@ -435,7 +439,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
         if (NS != 27 && !over)
         {
             // 7-point Laplacian: its stencil order, then the gradient pass over the 26 neighbours
-            seen = S.word[sl1][rec0] & 0xFFFFu;
+            uint32_t seen = own;
             const int nq = p.ns + p.ng;
             for (int q = 0; q < nq && !over; q++)
             {
