@@ -69,6 +69,7 @@ struct opgpu_ctx {
     long long wl_slice = 0;
     int2* d_bucket = nullptr;
     unsigned* d_bucket_count = nullptr;
+    unsigned* d_bucket_off = nullptr;
     long long bucket_cap = 0;
     int slice = 0;
     int variant = kVariantTiled;
@@ -454,6 +455,9 @@ extern "C" uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out)
         if (dalloc(&ctx->d_bucket_count, (size_t)(kListCap + 1) * nblocks) != cudaSuccess) return bail(OPGPU_E_CUDA);
         if (cudaMemset(ctx->d_bucket_count, 0, (kListCap + 1) * nblocks * sizeof(unsigned)) != cudaSuccess)
             return bail(OPGPU_E_CUDA);
+        if (dalloc(&ctx->d_bucket_off, (size_t)(kListCap + 1) * (nblocks + 1)) != cudaSuccess) return bail(OPGPU_E_CUDA);
+        if (cudaMemset(ctx->d_bucket_off, 0, (kListCap + 1) * (nblocks + 1) * sizeof(unsigned)) != cudaSuccess)
+            return bail(OPGPU_E_CUDA);
     }
     if (dalloc(&ctx->d_status, 1) != cudaSuccess) return bail(OPGPU_E_CUDA);
     if (dalloc(&ctx->d_counters, kNumCounters) != cudaSuccess) return bail(OPGPU_E_CUDA);
@@ -487,7 +491,7 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     dfree(ctx->d_slow_list);
     dfree(ctx->d_slow_count);
     dfree(ctx->d_wl);
-    dfree(ctx->d_bucket); dfree(ctx->d_bucket_count);
+    dfree(ctx->d_bucket); dfree(ctx->d_bucket_count); dfree(ctx->d_bucket_off);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
     for (auto& s : ctx->slots)
@@ -790,7 +794,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
         a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
-        a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
+        a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count; a.bucket_off = ctx->d_bucket_off;
         a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;
         LaunchInfo info;
         if (ctx->timing)
@@ -1245,7 +1249,7 @@ extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
     // state buffer, its volume sums and counters are discarded)
     a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
     a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
-    a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count;
+    a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count; a.bucket_off = ctx->d_bucket_off;
     a.bucket_cap = ctx->bucket_cap; a.slice = ctx->slice;
     const int nblocks = ctx->fp32 ? launch_classify_f32(sp, a, ctx->K, ctx->stream)
                                   : launch_classify_f64(sp, a, ctx->K, ctx->stream);

@@ -120,6 +120,8 @@ struct StepArrays {
     long long wl_slice;        // bytes per classify block
     int2* bucket;              // [kListCap + 1][bucket_cap] entries per list length, block-private slices
     unsigned* bucket_count;    // [kListCap + 1][max blocks] entries per slice
+    unsigned* bucket_off;      // [kListCap + 1][blocks + 1] exclusive prefix of bucket_count per list
+                               // length, then the length's total
     long long bucket_cap;
     int slice;                 // entries per classify-block slice
 };

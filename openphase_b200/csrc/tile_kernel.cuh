@@ -16,9 +16,10 @@
 //     - writes the list to the work buffer and appends the voxel to its block's slice of the
 //       bucket of its list length.
 // compute (list_compute_kernel<N>)
-//   One kernel per list length N = 2..kListCap, each CUDA block draining one classify block's
-//   slice: fully unrolled, register-only pair kinetics, driving force, projection, merge and
-//   finalize (the operation order of list_step), new record written to the output state.
+//   One kernel per list length N = 2..kListCap over all the slices' entries of that length (a
+//   small scan kernel turns the per-slice counts into offsets), split evenly over the CUDA blocks:
+//   fully unrolled, register-only pair kinetics, driving force, projection, merge and finalize
+//   (the operation order of list_step), new record written to the output state.
 // Lists longer than kListCap and voxels next to a grain without a window slot go to the general-path
 // worklist, processed one warp per voxel (warp_step.cuh).
 #pragma once
@@ -37,6 +38,7 @@ struct WindowSlots {
 constexpr int kSlotHash = 64;        // grain -> slot hash table entries
 constexpr int kTileVolSlots = 512;      // grain-volume hash of the compute kernels
 constexpr int kClassifyVolSlots = 256;  // grain-volume hash of the classify kernel (bulk voxels)
+constexpr int kComputeBlocks = 148 * 8; // blocks of each per-length compute kernel
 constexpr int kTileTY = kTileRows;   // tile rows (blocks of kTileZ x kTileRows threads)
 
 template <int TY>
@@ -491,39 +493,91 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     flush_block(a, wide, ein, eout, st, S.cnt, S.vol_key, S.vol_sum, kClassifyVolSlots, t, NT);
 }
 
+// Exclusive prefix of the per-slice bucket counts, one block per list length N = 2..kListCap:
+// bucket_off[N][s] = entries of length N in slices before s, bucket_off[N][nslices] = their total.
+static __global__ void __launch_bounds__(1024) bucket_scan_kernel(const StepArrays a, int nslices)
+{
+    __shared__ unsigned s_warp[32];
+    const int N = blockIdx.x + 2;
+    const unsigned* __restrict__ cnt = a.bucket_count + (long long)N * nslices;
+    unsigned* __restrict__ off = a.bucket_off + (long long)N * (nslices + 1);
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int per = (nslices + 1023) / 1024;
+    const int s0 = min(t * per, nslices), s1 = min(s0 + per, nslices);
+    unsigned sum = 0;
+    for (int s = s0; s < s1; s++) sum += cnt[s];
+    unsigned incl = sum;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0)
+    {
+        unsigned x = s_warp[lane];
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const unsigned u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += u;
+        }
+        s_warp[lane] = x;   // inclusive over warps
+    }
+    __syncthreads();
+    unsigned base = (w > 0 ? s_warp[w - 1] : 0u) + incl - sum;
+    for (int s = s0; s < s1; s++) { off[s] = base; base += cnt[s]; }
+    if (t == 0) off[nslices] = s_warp[31];
+}
+
 // Stages 2-5 for lists of exactly N fields (compile-time), all arrays in registers; the operation
-// order is that of list_step.  Each block drains one classify block's slice of bucket N.
+// order is that of list_step.  The entries of length N from all classify slices form one index
+// range (bucket_off); each CUDA block takes an equal contiguous part of it, its warps 32
+// consecutive entries at a time, so that no warp idles while another drains a long slice.
 template <class R, int N, int KS>
-__global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant__ StepParams p, const StepArrays a)
+__global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant__ StepParams p, const StepArrays a,
+                                                           int nslices)
 {
     constexpr int NP = N * (N - 1) / 2;
     __shared__ int s_key[kTileVolSlots];
     __shared__ double s_sum[kTileVolSlots];
     __shared__ unsigned long long s_cnt[3];
     const int t = threadIdx.x;
-    const unsigned cnt = a.bucket_count[N * (long long)gridDim.x + blockIdx.x];
-    if (cnt == 0) return;
+    const unsigned* __restrict__ off = a.bucket_off + (long long)N * (nslices + 1);
+    const unsigned total = off[nslices];
+    const unsigned per = ((total + gridDim.x * 32u - 1u) / (gridDim.x * 32u)) * 32u;
+    const unsigned r0 = blockIdx.x * per;
+    if (r0 >= total) return;
+    const unsigned r1 = min(total, r0 + per);
     for (int i = t; i < kTileVolSlots; i += blockDim.x) { s_key[i] = -1; s_sum[i] = 0.0; }
     if (t < 3) s_cnt[t] = 0ull;
     __syncthreads();
     const long long N_ = p.n;
-    const int2* __restrict__ list = a.bucket + (long long)N * a.bucket_cap + (long long)blockIdx.x * a.slice;
-    const unsigned char* __restrict__ wbase = a.wl + (long long)blockIdx.x * a.wl_slice;
+    const int2* __restrict__ buck = a.bucket + (long long)N * a.bucket_cap;
     constexpr int kPad = ((2 * N + 7) / 8) * 8;
     R* __restrict__ vout = static_cast<R*>(a.val_out);
     uint32_t st = 0;
     unsigned eout = 0;
     const unsigned lane = t & 31u;
-    for (unsigned base = t - lane; base < cnt; base += blockDim.x)   // the same trip count per warp
+    for (unsigned base = r0 + (t - lane); base < r1; base += blockDim.x)   // the same trip count per warp
     {
         const unsigned e = base + lane;
+        // slice of the warp's first entry (off[lo] <= base < off[hi]), then of each lane's entry
+        int lo = 0, hi = nslices;
+        while (hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (off[mid] <= base) lo = mid; else hi = mid;
+        }
         int vg[N];       // the voxel's contributions to the grain volumes (grain -1: none)
         double vw[N];
 #pragma unroll
         for (int i = 0; i < N; i++) { vg[i] = -1; vw[i] = 0.0; }
-        if (e < cnt)
+        if (e < r1)
         {
-        const int2 ent = list[e];
+        while (off[lo + 1] <= e) lo++;   // off[nslices] = total > e
+        const int2 ent = buck[(long long)lo * a.slice + (e - off[lo])];
+        const unsigned char* __restrict__ wbase = a.wl + (long long)lo * a.wl_slice;
         const long long v = ent.x & 0x7fffffff;
         const int flag = (ent.x >> 31) ? 2 : 1;
         const int16_t* __restrict__ rg = reinterpret_cast<const int16_t*>(wbase + ent.y);
@@ -807,13 +861,14 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
         e = cudaEventRecord(static_cast<cudaEvent_t>(info->after_classify), s);
         if (e != cudaSuccess) return (int)e;
     }
-    list_compute_kernel<R, 2, KS><<<nblocks, 128, 0, s>>>(p, a);
-    list_compute_kernel<R, 3, KS><<<nblocks, 128, 0, s>>>(p, a);
-    list_compute_kernel<R, 4, KS><<<nblocks, 128, 0, s>>>(p, a);
-    list_compute_kernel<R, 5, KS><<<nblocks, 128, 0, s>>>(p, a);
-    list_compute_kernel<R, 6, KS><<<nblocks, 128, 0, s>>>(p, a);
-    list_compute_kernel<R, 7, KS><<<nblocks, 128, 0, s>>>(p, a);
-    list_compute_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a);
+    bucket_scan_kernel<<<kListCap - 1, 1024, 0, s>>>(a, nblocks);
+    list_compute_kernel<R, 2, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 3, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 4, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 5, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 6, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 7, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 8, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
     // general path: one warp per voxel of the worklist
     {
         auto gk = warp_general_kernel<R, KS, KL>;
@@ -822,7 +877,7 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
         if (e != cudaSuccess) return (int)e;
         gk<<<148 * 4, 128, wsm, s>>>(p, a);
     }
-    if (info) info->kernels += 9;
+    if (info) info->kernels += 10;
     return (int)cudaGetLastError();
 }
 
