@@ -530,6 +530,21 @@ static __global__ void __launch_bounds__(1024) bucket_scan_kernel(const StepArra
     if (t == 0) off[nslices] = s_warp[31];
 }
 
+// Slice of entry e of one list length: the s with off[s] <= e < off[s + 1] (off[nslices] > e).
+__device__ __forceinline__ int slice_of(const unsigned* __restrict__ off, int nslices, unsigned e)
+{
+    int lo = 0, hi = nslices;
+    while (hi - lo > 1)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= e) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+constexpr int kChunkTable = 128;   // 32-entry chunks of a compute block whose slices are tabulated
+constexpr int kVolCache = 4;       // per-thread grain-volume cache of the compute kernels
+
 // Stages 2-5 for lists of exactly N fields (compile-time), all arrays in registers; the operation
 // order is that of list_step.  The entries of length N from all classify slices form one index
 // range (bucket_off); each CUDA block takes an equal contiguous part of it, its warps 32
@@ -542,6 +557,7 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     __shared__ int s_key[kTileVolSlots];
     __shared__ double s_sum[kTileVolSlots];
     __shared__ unsigned long long s_cnt[3];
+    __shared__ int s_chunk[kChunkTable];
     const int t = threadIdx.x;
     const unsigned* __restrict__ off = a.bucket_off + (long long)N * (nslices + 1);
     const unsigned total = off[nslices];
@@ -551,9 +567,20 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     const unsigned r1 = min(total, r0 + per);
     for (int i = t; i < kTileVolSlots; i += blockDim.x) { s_key[i] = -1; s_sum[i] = 0.0; }
     if (t < 3) s_cnt[t] = 0ull;
+    // slice of each 32-entry chunk of the block's range
+    const unsigned nchunks = (r1 - r0 + 31u) / 32u;
+    const bool tabulated = nchunks <= (unsigned)kChunkTable;
+    if (tabulated)
+        for (unsigned c = t; c < nchunks; c += blockDim.x) s_chunk[c] = slice_of(off, nslices, r0 + 32u * c);
     __syncthreads();
     const long long N_ = p.n;
     const int2* __restrict__ buck = a.bucket + (long long)N * a.bucket_cap;
+    // grain-volume contributions of this thread's voxels, most recent grain first (consecutive
+    // voxels of a thread lie close together and mostly share their grains)
+    int cg[kVolCache];
+    double cv[kVolCache];
+#pragma unroll
+    for (int c = 0; c < kVolCache; c++) { cg[c] = -1; cv[c] = 0.0; }
     constexpr int kPad = ((2 * N + 7) / 8) * 8;
     R* __restrict__ vout = static_cast<R*>(a.val_out);
     uint32_t st = 0;
@@ -562,17 +589,8 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     for (unsigned base = r0 + (t - lane); base < r1; base += blockDim.x)   // the same trip count per warp
     {
         const unsigned e = base + lane;
-        // slice of the warp's first entry (off[lo] <= base < off[hi]), then of each lane's entry
-        int lo = 0, hi = nslices;
-        while (hi - lo > 1)
-        {
-            const int mid = (lo + hi) >> 1;
-            if (off[mid] <= base) lo = mid; else hi = mid;
-        }
-        int vg[N];       // the voxel's contributions to the grain volumes (grain -1: none)
-        double vw[N];
-#pragma unroll
-        for (int i = 0; i < N; i++) { vg[i] = -1; vw[i] = 0.0; }
+        // slice of the warp's first entry, then of each lane's entry
+        int lo = tabulated ? s_chunk[(base - r0) >> 5] : slice_of(off, nslices, base);
         if (e < r1)
         {
         while (off[lo + 1] <= e) lo++;   // off[nslices] = total > e
@@ -816,7 +834,24 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
                 if (!isfinite((double)w)) st |= kStNonFinite;
                 a.idx_out[pos * N_ + v] = (int16_t)g[i];
                 vout[pos * N_ + v] = w;
-                if (in_volume_window(p, v)) { vg[i] = g[i]; vw[i] = (double)w; }
+                if (in_volume_window(p, v))
+                {
+                    const int gi = g[i];
+                    const double wi = (double)w;
+                    bool hit = false;
+#pragma unroll
+                    for (int c = 0; c < kVolCache; c++)
+                        if (cg[c] == gi) { cv[c] += wi; hit = true; }
+                    if (!hit)
+                    {
+                        if (cg[kVolCache - 1] >= 0)
+                            vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, cg[kVolCache - 1], cv[kVolCache - 1]);
+#pragma unroll
+                        for (int c = kVolCache - 1; c > 0; c--) { cg[c] = cg[c - 1]; cv[c] = cv[c - 1]; }
+                        cg[0] = gi;
+                        cv[0] = wi;
+                    }
+                }
                 pos++;
             }
         }
@@ -825,19 +860,10 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
         a.cnt_out[v] = (uint8_t)pos;
         eout += pos;
         }
-        // one shared-memory add per grain and warp: the lanes adding to the same grain sum first
-#pragma unroll
-        for (int i = 0; i < N; i++)
-        {
-            const unsigned peers = __match_any_sync(0xffffffffu, vg[i]);
-            if (vg[i] >= 0)
-            {
-                double s = 0.0;
-                for (unsigned mk = peers; mk; mk &= mk - 1u) s += __shfl_sync(peers, vw[i], __ffs(mk) - 1);
-                if (lane == (unsigned)(__ffs(peers) - 1)) vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, vg[i], s);
-            }
-        }
     }
+#pragma unroll
+    for (int c = 0; c < kVolCache; c++)
+        if (cg[c] >= 0) vol_insert_n(s_key, s_sum, kTileVolSlots, a.vol_acc, cg[c], cv[c]);
     flush_block(a, 0u, 0u, eout, st, s_cnt, s_key, s_sum, kTileVolSlots, t, blockDim.x);
 }
 
