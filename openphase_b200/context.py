@@ -122,13 +122,23 @@ class Context:
         _check(lib().opgpu_total_entries(self.h, C.byref(t)), self.h, "total_entries")
         return t.value
 
-    def download(self):
+    def download(self, out=None):
+        """Ragged host copy of the state: counts[N], then (index, value) pairs in voxel order.
+
+        `out` may give (counts int32[N], idx int32[>= total], val float64[>= total]) arrays to fill,
+        e.g. pinned host memory; the arrays returned are then views trimmed to the entry count."""
         total = self.total_entries()
-        counts = np.empty(self.n, dtype=np.int32)
-        idx = np.empty(total, dtype=np.int32)
-        val = np.empty(total, dtype=np.float64)
+        if out is None:
+            counts = np.empty(self.n, dtype=np.int32)
+            idx = np.empty(total, dtype=np.int32)
+            val = np.empty(total, dtype=np.float64)
+        else:
+            counts, idx, val = out
+            if (counts.dtype != np.int32 or idx.dtype != np.int32 or val.dtype != np.float64 or counts.size != self.n
+                    or idx.size < total or val.size < total or not all(a.flags.c_contiguous for a in out)):
+                raise ValueError("download: out must be contiguous int32[N], int32[>=total], float64[>=total]")
         _check(lib().opgpu_download_lists(self.h, ptr(counts), ptr(idx), ptr(val)), self.h, "download_lists")
-        return counts, idx, val
+        return counts, idx[:total], val[:total]
 
     def flags(self):
         f = np.empty(self.n, dtype=np.int8)

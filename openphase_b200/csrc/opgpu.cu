@@ -680,40 +680,93 @@ extern "C" uint32_t opgpu_set_orientations(opgpu_ctx* ctx, const double* quat)
     return OPGPU_OK;
 }
 
+// Device scratch of the list upload / download / entry count, carved from the spare ping-pong
+// state buffers (they hold no state between calls: every step rewrites them); a piece that does
+// not fit there is allocated for the call and freed with the scratch.
+struct IoScratch {
+    unsigned char* a;   // spare value planes
+    size_t a_left;
+    unsigned char* b;   // spare index planes
+    size_t b_left;
+    std::vector<void*> owned;
+
+    IoScratch(opgpu_ctx* ctx, int spare)
+        : a(static_cast<unsigned char*>(ctx->val[spare])), a_left((size_t)ctx->n * ctx->K * ctx->rsz),
+          b(reinterpret_cast<unsigned char*>(ctx->idx[spare])), b_left((size_t)ctx->n * ctx->K * sizeof(int16_t))
+    {
+    }
+    ~IoScratch()
+    {
+        for (void* p : owned) cudaFree(p);
+    }
+    IoScratch(const IoScratch&) = delete;
+    IoScratch& operator=(const IoScratch&) = delete;
+
+    template <class T>
+    cudaError_t take(T** p, size_t count, bool prefer_a)
+    {
+        const size_t bytes = ((count * sizeof(T) + 16 + 255) / 256) * 256;   // bases stay 256-byte aligned
+        for (int pass = 0; pass < 2; pass++)
+        {
+            const bool use_a = (pass == 0) == prefer_a;
+            unsigned char*& base = use_a ? a : b;
+            size_t& left = use_a ? a_left : b_left;
+            if (bytes <= left)
+            {
+                *p = reinterpret_cast<T*>(base);
+                base += bytes;
+                left -= bytes;
+                return cudaSuccess;
+            }
+        }
+        void* q = nullptr;
+        const cudaError_t e = cudaMalloc(&q, bytes);
+        if (e != cudaSuccess) return e;
+        owned.push_back(q);
+        *p = static_cast<T*>(q);
+        return cudaSuccess;
+    }
+};
+
 extern "C" uint32_t opgpu_upload_lists(opgpu_ctx* ctx, const int32_t* counts, const int32_t* idx, const double* val)
 {
     if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_upload_lists: call opgpu_set_grains first")) return r;
     if (!counts || !idx || !val) return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: null array");
     const long long N = ctx->n;
     long long total = 0;
+    int bad = 0;
+#pragma omp parallel for reduction(+ : total) reduction(| : bad)
     for (long long v = 0; v < N; v++)
     {
-        if (counts[v] < 0 || counts[v] > 64)
-            return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: a voxel list must hold 0..64 entries");
+        if (counts[v] < 0 || counts[v] > 64) bad |= 1;
         total += counts[v];
     }
+    if (bad) return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: a voxel list must hold 0..64 entries");
+    const int G = ctx->G;
+#pragma omp parallel for reduction(| : bad)
     for (long long q = 0; q < total; q++)
-        if (idx[q] < 0 || idx[q] >= ctx->G) return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: grain index out of range");
+        if (idx[q] < 0 || idx[q] >= G) bad |= 2;
+    if (bad) return fail(ctx, OPGPU_E_INVALID, "opgpu_upload_lists: grain index out of range");
     int32_t *d_counts = nullptr, *d_idx = nullptr;
     long long *d_off = nullptr, *d_wide = nullptr;
     double* d_val = nullptr;
-    void* d_tmp = nullptr;
+    unsigned char* d_tmp = nullptr;
     size_t tmp_bytes = 0;
     uint32_t rc = OPGPU_OK;
-    auto cleanup = [&]() { dfree(d_counts); dfree(d_idx); dfree(d_off); dfree(d_wide); dfree(d_val); dfree(d_tmp); };
+    IoScratch scr(ctx, 1);   // the state is loaded into buffer 0
+    cudaError_t e = cudaSuccess;
     do {
-        cudaError_t e;
-        if ((e = dalloc(&d_counts, N)) != cudaSuccess) break;
-        if ((e = dalloc(&d_off, N)) != cudaSuccess) break;
-        if ((e = dalloc(&d_wide, N)) != cudaSuccess) break;
-        if ((e = dalloc(&d_idx, total)) != cudaSuccess) break;
-        if ((e = dalloc(&d_val, total)) != cudaSuccess) break;
+        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_wide, d_off, N, ctx->stream)) != cudaSuccess) break;
+        if ((e = scr.take(&d_val, total, true)) != cudaSuccess) break;
+        if ((e = scr.take(&d_idx, total, true)) != cudaSuccess) break;
+        if ((e = scr.take(&d_off, N, false)) != cudaSuccess) break;
+        if ((e = scr.take(&d_wide, N, false)) != cudaSuccess) break;
+        if ((e = scr.take(&d_counts, N, false)) != cudaSuccess) break;
+        if ((e = scr.take(&d_tmp, tmp_bytes, false)) != cudaSuccess) break;
         if ((e = cudaMemcpyAsync(d_counts, counts, N * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) break;
         if ((e = cudaMemcpyAsync(d_idx, idx, total * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) break;
         if ((e = cudaMemcpyAsync(d_val, val, total * sizeof(double), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) break;
         widen_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, d_counts, d_wide);
-        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_wide, d_off, N, ctx->stream)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&d_tmp, tmp_bytes + 16)) != cudaSuccess) break;
         if ((e = cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_wide, d_off, N, ctx->stream)) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(ctx->d_vol_acc, 0, ctx->G * sizeof(double), ctx->stream)) != cudaSuccess) break;
         const int cur = 0;
@@ -728,13 +781,9 @@ extern "C" uint32_t opgpu_upload_lists(opgpu_ctx* ctx, const int32_t* counts, co
         ctx->cur = cur;
         ctx->state_loaded = true;
         ctx->initialized = false;
-        e = cudaSuccess;
-        if (e != cudaSuccess) break;
-        cleanup();
         return OPGPU_OK;
     } while (0);
-    rc = fail(ctx, OPGPU_E_CUDA, std::string("opgpu_upload_lists: ") + cudaGetErrorString(cudaGetLastError()));
-    cleanup();
+    rc = fail(ctx, OPGPU_E_CUDA, std::string("opgpu_upload_lists: ") + cudaGetErrorString(e));
     return rc;
 }
 
@@ -861,19 +910,19 @@ extern "C" uint32_t opgpu_total_entries(opgpu_ctx* ctx, int64_t* total)
     const long long N = ctx->n;
     int32_t* d_counts = nullptr;
     long long *d_sum = nullptr, *d_wide = nullptr;
-    void* d_tmp = nullptr;
+    unsigned char* d_tmp = nullptr;
     size_t tmp_bytes = 0;
-    CK(dalloc(&d_counts, N));
-    CK(dalloc(&d_wide, N));
-    CK(dalloc(&d_sum, 1));
-    counts_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], d_counts, d_wide);
+    IoScratch scr(ctx, 1 - ctx->cur);
     CK(cub::DeviceReduce::Sum(nullptr, tmp_bytes, d_wide, d_sum, N, ctx->stream));
-    CK(cudaMalloc(&d_tmp, tmp_bytes + 16));
+    CK(scr.take(&d_counts, N, false));
+    CK(scr.take(&d_wide, N, false));
+    CK(scr.take(&d_sum, 1, false));
+    CK(scr.take(&d_tmp, tmp_bytes, false));
+    counts_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], d_counts, d_wide);
     CK(cub::DeviceReduce::Sum(d_tmp, tmp_bytes, d_wide, d_sum, N, ctx->stream));
     long long t = 0;
     CK(cudaMemcpyAsync(&t, d_sum, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    dfree(d_counts); dfree(d_wide); dfree(d_sum); dfree(d_tmp);
     *total = t;
     return OPGPU_OK;
 }
@@ -888,16 +937,17 @@ extern "C" uint32_t opgpu_download_lists(opgpu_ctx* ctx, int32_t* counts, int32_
     int32_t *d_counts = nullptr, *d_idx = nullptr;
     long long *d_off = nullptr, *d_wide = nullptr;
     double* d_val = nullptr;
-    void* d_tmp = nullptr;
+    unsigned char* d_tmp = nullptr;
     size_t tmp_bytes = 0;
-    CK(dalloc(&d_counts, N));
-    CK(dalloc(&d_off, N));
-    CK(dalloc(&d_wide, N));
-    CK(dalloc(&d_idx, total));
-    CK(dalloc(&d_val, total));
-    counts_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], d_counts, d_wide);
+    IoScratch scr(ctx, 1 - ctx->cur);
     CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_wide, d_off, N, ctx->stream));
-    CK(cudaMalloc(&d_tmp, tmp_bytes + 16));
+    CK(scr.take(&d_val, total, true));
+    CK(scr.take(&d_idx, total, true));
+    CK(scr.take(&d_off, N, false));
+    CK(scr.take(&d_wide, N, false));
+    CK(scr.take(&d_counts, N, false));
+    CK(scr.take(&d_tmp, tmp_bytes, false));
+    counts_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], d_counts, d_wide);
     CK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_wide, d_off, N, ctx->stream));
     if (ctx->fp32)
         gather_kernel<float><<<grid_for(N, 256), 256, 0, ctx->stream>>>(N, ctx->cnt[ctx->cur], ctx->idx[ctx->cur],
@@ -910,7 +960,6 @@ extern "C" uint32_t opgpu_download_lists(opgpu_ctx* ctx, int32_t* counts, int32_
     CK(cudaMemcpyAsync(idx, d_idx, total * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(val, d_val, total * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    dfree(d_counts); dfree(d_off); dfree(d_wide); dfree(d_idx); dfree(d_val); dfree(d_tmp);
     return OPGPU_OK;
 }
 
