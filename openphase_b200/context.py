@@ -44,7 +44,10 @@ class Context:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:   # interpreter shutdown: the library module may already be torn down
+            pass
 
     def __enter__(self):
         return self

@@ -860,15 +860,22 @@ __global__ void adjoint_bulk_kernel(const __grid_constant__ StepParams p, const 
 // and Laplacians the forward step used; own fields are the leading nonzero values).
 template <class R, int N, int KS>
 __global__ void __launch_bounds__(128) adjoint_list_kernel(const __grid_constant__ StepParams p, const StepArrays a,
-                                                            const AdjArrays aa)
+                                                            const AdjArrays aa, int nslices)
 {
-    const unsigned cnt = a.bucket_count[N * (long long)gridDim.x + blockIdx.x];
-    const int2* __restrict__ list = a.bucket + (long long)N * a.bucket_cap + (long long)blockIdx.x * a.slice;
-    const unsigned char* __restrict__ wbase = a.wl + (long long)blockIdx.x * a.wl_slice;
+    // the entries of length N from all classify slices form one index range, split evenly
+    const unsigned* __restrict__ off = a.bucket_off + (long long)N * (nslices + 1);
+    const unsigned total = off[nslices];
+    const unsigned per = ((total + gridDim.x * 32u - 1u) / (gridDim.x * 32u)) * 32u;
+    const unsigned r0 = blockIdx.x * per;
+    if (r0 >= total) return;
+    const unsigned r1 = min(total, r0 + per);
+    const int2* __restrict__ buck = a.bucket + (long long)N * a.bucket_cap;
     constexpr int kPad = ((2 * N + 7) / 8) * 8;
-    for (unsigned e = threadIdx.x; e < cnt; e += blockDim.x)
+    for (unsigned e = r0 + threadIdx.x; e < r1; e += blockDim.x)
     {
-        const int2 ent = list[e];
+        const int sl = slice_of(off, nslices, e);
+        const int2 ent = buck[(long long)sl * a.slice + (e - off[sl])];
+        const unsigned char* __restrict__ wbase = a.wl + (long long)sl * a.wl_slice;
         const long long v = ent.x & 0x7fffffff;
         const int flag = (ent.x >> 31) ? 2 : 1;
         const int16_t* __restrict__ rg = reinterpret_cast<const int16_t*>(wbase + ent.y);
@@ -962,16 +969,18 @@ int launch_tlm_step(const StepParams& p, const StepArrays& a, const AdjArrays& a
     return (int)cudaGetLastError();
 }
 
+constexpr int kAdjListBlocks = 148 * 8;   // blocks of each per-length adjoint kernel
+
 template <class R, int KS>
 static void adjoint_kernels(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int nblocks, cudaStream_t s)
 {
-    adjoint_list_kernel<R, 2, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
-    adjoint_list_kernel<R, 3, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
-    adjoint_list_kernel<R, 4, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
-    adjoint_list_kernel<R, 5, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
-    adjoint_list_kernel<R, 6, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
-    adjoint_list_kernel<R, 7, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
-    adjoint_list_kernel<R, 8, KS><<<nblocks, 128, 0, s>>>(p, a, aa);
+    adjoint_list_kernel<R, 2, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
+    adjoint_list_kernel<R, 3, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
+    adjoint_list_kernel<R, 4, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
+    adjoint_list_kernel<R, 5, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
+    adjoint_list_kernel<R, 6, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
+    adjoint_list_kernel<R, 7, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
+    adjoint_list_kernel<R, 8, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
     adjoint_worklist_kernel<R, KS><<<148 * 4, 64, 0, s>>>(p, a, aa);
 }
 

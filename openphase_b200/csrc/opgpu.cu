@@ -1308,7 +1308,7 @@ extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
     CK(cudaMemsetAsync(ctx->d_counters + kCntCrowdedLast, 0, sizeof(unsigned long long), ctx->stream));
     if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, nblocks, lam0, ctx->stream))
         return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: launch");
-    ctx->kernel_launches += 11;
+    ctx->kernel_launches += 12;
     ctx->lam_cur = 1 - ctx->lam_cur;
     // the state before the step becomes the current state (the adjoint is aligned with it)
     if (uint32_t r = copy_state(ctx, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur], s.cnt, s.idx, s.val)) return r;

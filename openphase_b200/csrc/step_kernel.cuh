@@ -66,6 +66,19 @@ __device__ __forceinline__ double limited_force(const StepParams& p, const StepA
     return locdG;
 }
 
+// Slice of entry e of one list length in the concatenated length buckets: the s with
+// off[s] <= e < off[s + 1] (off[nslices] > e).
+__device__ __forceinline__ int slice_of(const unsigned* __restrict__ off, int nslices, unsigned e)
+{
+    int lo = 0, hi = nslices;
+    while (hi - lo > 1)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= e) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // Per-block grain-volume table in shared memory.
 constexpr int kVolSlots = 1024;
 

@@ -530,18 +530,6 @@ static __global__ void __launch_bounds__(1024) bucket_scan_kernel(const StepArra
     if (t == 0) off[nslices] = s_warp[31];
 }
 
-// Slice of entry e of one list length: the s with off[s] <= e < off[s + 1] (off[nslices] > e).
-__device__ __forceinline__ int slice_of(const unsigned* __restrict__ off, int nslices, unsigned e)
-{
-    int lo = 0, hi = nslices;
-    while (hi - lo > 1)
-    {
-        const int mid = (lo + hi) >> 1;
-        if (off[mid] <= e) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
 constexpr int kChunkTable = 128;   // 32-entry chunks of a compute block whose slices are tabulated
 constexpr int kVolCache = 4;       // per-thread grain-volume cache of the compute kernels
 
@@ -907,8 +895,8 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
     return (int)cudaGetLastError();
 }
 
-// The classify kernel alone (work records, length buckets, general-path worklist, bulk copies):
-// the adjoint reverses the lists it leaves.  Returns the number of classify blocks (the slices of
+// The classify kernel and the bucket scan (work records, length buckets and their offsets,
+// general-path worklist, bulk copies): the adjoint reverses the lists they leave.  Returns the number of classify blocks (the slices of
 // the buckets) or a negative error.
 template <class R, int KS, int NS>
 int launch_classify_ns(const StepParams& p, const StepArrays& a, void* stream)
@@ -924,6 +912,7 @@ int launch_classify_ns(const StepParams& p, const StepArrays& a, void* stream)
     e = cudaMemsetAsync(a.slow_count, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return -(int)e;
     kern<<<dim3(gz, gy, gx), dim3(kTileZ, kTileTY), smem, s>>>(p, a, xchunk);
+    bucket_scan_kernel<<<kListCap - 1, 1024, 0, s>>>(a, gz * gy * gx);
     e = cudaGetLastError();
     return e == cudaSuccess ? gz * gy * gx : -(int)e;
 }
