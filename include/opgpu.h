@@ -79,7 +79,12 @@ typedef struct opgpu_model {
     double  nucleus_volume_factor;   /* default 1.0                                               */
     /* Anisotropic interface energy (InterfaceEnergyModel.h:78-94, 325-345; InterfaceProperties.cpp:
      * 617-673); any may be NULL (all ISO, all phases solid). */
-    const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC ($EnergyModel_a_b)                 */
+    const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC, 2 = DISORIENTATION ($EnergyModel_a_b;
+                                      DISORIENTATION: InterfaceEnergyModel.h:303-323, the energy of
+                                      a grain pair from the cubic disorientation of the two grains'
+                                      orientations (opgpu_set_orientations), tabulated per grain pair;
+                                      its Energy and MaxEnergy are 0 as in the reference, so with
+                                      $Limiting on the driving force of such pairs is limited to 0) */
     const double* cubic_eps;       /* [P*P] CUBIC strength ($EpsilonE_a_b)                        */
     const int32_t* phase_solid;    /* [P] 1 = Solid, 0 = Liquid ($State_p); anisotropy weights
                                       only count solid grains                                     */

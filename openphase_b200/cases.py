@@ -53,6 +53,8 @@ class Case:
     init: str = "voronoi"                      # "voronoi" or "nuclei" (grain 0 = matrix)
     nucleus_radius: float = 4.0
     orientations: bool = False                 # random unit quaternion per grain
+    orientation_spread: float = 0.0            # > 0: rotations by at most this angle (rad) instead
+    disorientation: bool = False               # DISORIENTATION energy model for every phase pair
 
     @property
     def n(self) -> int:
@@ -78,7 +80,9 @@ class Case:
         return np.array(self.phase_cubic_eps, dtype=np.float64) if self.phase_cubic_eps else None
 
     def energy_models(self) -> Optional[np.ndarray]:
-        """P x P model codes: 0 ISO, 1 CUBIC."""
+        """P x P model codes: 0 ISO, 1 CUBIC, 2 DISORIENTATION."""
+        if self.disorientation:
+            return np.full((self.nphases, self.nphases), 2, dtype=np.int32)
         e = self.cubic_eps()
         return None if e is None else (e != 0.0).astype(np.int32)
 
@@ -89,7 +93,11 @@ class Case:
         return g
 
     def quaternions(self) -> Optional[np.ndarray]:
-        return init.quaternions(self.ngrains, self.seed) if self.orientations else None
+        if not self.orientations:
+            return None
+        if self.orientation_spread > 0.0:
+            return init.small_rotations(self.ngrains, self.seed, self.orientation_spread)
+        return init.quaternions(self.ngrains, self.seed)
 
     def initial_state(self, threads: int = 0):
         if self.init == "nuclei":

@@ -60,6 +60,11 @@ struct opgpu_ctx {
     int lam_cur = 0, dphi_cur = 0;
     bool adjoint_ready = false, tlm_ready = false;
     bool dg_pair_dirty = true;
+    // DISORIENTATION energies: per-grain-pair table built on the host from the orientations
+    std::vector<int16_t> h_gphase;      // [G] phase of every grain
+    std::vector<double> h_quat;         // [G*4] orientations (s, x, y, z) as given; empty: unrotated
+    std::vector<double> h_user_sigma;   // [G*G] energies given to opgpu_set_pair_table; empty: none
+    bool pair_energy_dirty = true;
     uint32_t* d_status = nullptr;
     unsigned long long* d_counters = nullptr;
     int* d_slow_list = nullptr;      // overflow worklist of the tiled kernel (capacity N)
@@ -290,6 +295,47 @@ void free_grains(opgpu_ctx* c)
     c->d_gphase = nullptr; c->d_gstage = c->d_exist = nullptr;
     c->d_dg = c->d_pair_sigma = c->d_pair_mu = c->d_dg_pair = nullptr;
     c->dg_pair_dirty = true;
+    c->h_quat.clear();
+    c->h_user_sigma.clear();
+    c->pair_energy_dirty = true;
+}
+
+// Tools::getDisorientationCubic (src/Tools.cpp:626-678): rotation angle 2*acos(max |c|) of
+// dQ = A * B.inverted() over the 24 component combinations c of the cubic group (Grimmer 1974),
+// with the reference's factors 0.707 and 0.5; quaternion product and inverse as
+// include/Containers/Quaternion.h:257-266, 313-339 (component 0 = s).  Host code, so that log and
+// acos are the host library's, as in the reference.
+double disorientation_cubic(const double* A, const double* B)
+{
+    const double bs = B[0], bx = B[1], by = B[2], bz = B[3];
+    const double n2 = bs * bs + (bx * bx + by * by + bz * bz);
+    const double is = bs / n2, ix = (bx * (-1.0)) / n2, iy = (by * (-1.0)) / n2, iz = (bz * (-1.0)) / n2;
+    const double as = A[0], ax = A[1], ay = A[2], az = A[3];
+    const double d1 = ax * is + ay * iz - az * iy + as * ix;
+    const double d2 = -ax * iz + ay * is + az * ix + as * iy;
+    const double d3 = ax * iy - ay * ix + az * is + as * iz;
+    const double d0 = -ax * ix - ay * iy - az * iz + as * is;
+    const double c[24] = {
+        d0, d1, d2, d3,
+        (d0 + d1) * 0.707, (d0 - d1) * 0.707, (d2 + d3) * 0.707, (d2 - d3) * 0.707,
+        (d0 + d2) * 0.707, (d0 - d2) * 0.707, (d1 + d3) * 0.707, (d1 - d3) * 0.707,
+        (d0 + d3) * 0.707, (d0 - d3) * 0.707, (d1 + d2) * 0.707, (d1 - d2) * 0.707,
+        (d0 + d1 + d2 + d3) * 0.5, (d0 + d1 - d2 - d3) * 0.5, (d0 - d1 + d2 - d3) * 0.5, (d0 - d1 - d2 + d3) * 0.5,
+        (d0 + d1 + d2 - d3) * 0.5, (d0 + d1 - d2 + d3) * 0.5, (d0 - d1 + d2 + d3) * 0.5, (d0 - d1 - d2 - d3) * 0.5};
+    double m = 0.0;
+    for (int k = 0; k < 24; k++)
+        if (m < std::fabs(c[k])) m = std::fabs(c[k]);
+    return 2 * std::acos(m);
+}
+
+// InterfaceEnergyModel::CalculateDisorientation (include/InterfaceProperties/InterfaceEnergyModel.h:
+// 308-323): Read-Shockley-type energy of the disorientation angle, constant above 0.349066 rad.
+double disorientation_energy(const double* A, const double* B)
+{
+    const double constant = 0.85;
+    const double mis = disorientation_cubic(A, B);
+    if (mis <= 0.349066) return mis * constant * (0.8 - std::log(mis));
+    return 0.349066 * constant * (0.8 - std::log(0.349066));
 }
 
 // Grain counts up to which the limited driving force is tabulated per grain pair (8 * G^2 bytes).
@@ -529,23 +575,29 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         sp.mu_p[q] = m->mu[q];
         const double lim = m->limit ? m->limit[q] : 0.95;   // src/DrivingForce.cpp:161
         const int model = m->energy_model ? m->energy_model[q] : 0;
-        if (model < 0 || model > 1) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) or 1 (CUBIC)");
+        if (model < 0 || model > 2)
+            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO), 1 (CUBIC) or 2 (DISORIENTATION)");
         sp.emodel[q] = (signed char)model;
         sp.eps_p[q] = (model == 1 && m->cubic_eps) ? m->cubic_eps[q] : 0.0;
+        // DISORIENTATION reads no $Sigma: its Energy and MaxEnergy keep the constructor's 0
+        // (InterfaceEnergyModel.h:63-70, 303-306), which the triple-junction term and the
+        // driving-force limiter use
+        if (model == 2) sp.sigma_p[q] = 0.0;
         // MaxEnergy: Energy for ISO (InterfaceEnergyModel.h:82), Energy*(1 + Epsilon*1.41) for CUBIC
-        // (ReadInputCubic, InterfaceEnergyModel.h:87-94)
-        sp.maxe_p[q] = model == 1 ? m->sigma[q] * (1.0 + sp.eps_p[q] * 1.41) : m->sigma[q];
+        // (ReadInputCubic, InterfaceEnergyModel.h:87-94), 0 for DISORIENTATION
+        sp.maxe_p[q] = model == 1 ? m->sigma[q] * (1.0 + sp.eps_p[q] * 1.41) : (model == 2 ? 0.0 : m->sigma[q]);
         // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor
         double allowed = lim * sp.pref_df * sp.maxe_p[q];
         allowed *= m->regularization;
         sp.allowed_p[q] = allowed;
     }
-    sp.aniso = 0;
-    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] != 0;
+    sp.aniso = 0;   // models of the interface normal (the disorientation energy depends on the grain pair only)
+    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1;
     for (int a = 0; a < P; a++) sp.solid_p[a] = (signed char)(m->phase_solid ? (m->phase_solid[a] != 0) : 1);
     ctx->nvf = m->nucleus_volume_factor > 0.0 ? m->nucleus_volume_factor : 1.0;
     ctx->model_set = true;
     ctx->dg_pair_dirty = true;
+    ctx->pair_energy_dirty = true;
     return OPGPU_OK;
 }
 
@@ -587,6 +639,7 @@ extern "C" uint32_t opgpu_set_grains(opgpu_ctx* ctx, int32_t ngrains, const int3
     CK(cudaMemcpy(ctx->d_maxvol, zeros.data(), G * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_vol_acc, zeros.data(), G * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_gphase, gp.data(), G * sizeof(int16_t), cudaMemcpyHostToDevice));
+    ctx->h_gphase = gp;
     CK(cudaMemcpy(ctx->d_gstage, gs.data(), G * sizeof(int8_t), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_exist, ex.data(), G * sizeof(int8_t), cudaMemcpyHostToDevice));
     CK(dalloc(&ctx->d_grot, (size_t)G * 9));
@@ -607,10 +660,13 @@ extern "C" uint32_t opgpu_set_pair_table(opgpu_ctx* ctx, const double* sigma, co
     const size_t GG = (size_t)ctx->G * ctx->G;
     dfree(ctx->d_pair_sigma); ctx->d_pair_sigma = nullptr;
     dfree(ctx->d_pair_mu); ctx->d_pair_mu = nullptr;
+    ctx->h_user_sigma.clear();
+    ctx->pair_energy_dirty = true;
     if (sigma)
     {
         CK(dalloc(&ctx->d_pair_sigma, GG));
         CK(cudaMemcpy(ctx->d_pair_sigma, sigma, GG * sizeof(double), cudaMemcpyHostToDevice));
+        ctx->h_user_sigma.assign(sigma, sigma + GG);
     }
     if (mu)
     {
@@ -625,6 +681,7 @@ extern "C" uint32_t opgpu_set_pair_hash(opgpu_ctx* ctx, uint64_t seed, double lo
 {
     if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_set_pair_hash: call opgpu_set_grains first")) return r;
     ctx->sp.pair_mode = OPGPU_PAIRS_HASH;
+    ctx->pair_energy_dirty = true;
     ctx->sp.hash_seed = seed;
     ctx->sp.hash_lo = lo;
     ctx->sp.hash_span = span;
@@ -677,6 +734,47 @@ extern "C" uint32_t opgpu_set_orientations(opgpu_ctx* ctx, const double* quat)
         R[8] = 1.0 - 2.0 * (V0 * V0 + V1 * V1);
     }
     CK(cudaMemcpy(ctx->d_grot, rot.data(), rot.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (quat) ctx->h_quat.assign(quat, quat + 4 * (size_t)G);
+    else ctx->h_quat.clear();
+    ctx->pair_energy_dirty = true;
+    return OPGPU_OK;
+}
+
+// Per-grain-pair energies of the DISORIENTATION model (InterfaceProperties::SetSR,
+// src/InterfaceProperties.cpp:629-634): the energy of a pair depends on the two grains'
+// orientations only, so it is tabulated once (G*G, with the other phase pairs' values from the
+// user table or the phase model) and the step reads it as a per-grain-pair table.
+uint32_t refresh_pair_energy(opgpu_ctx* ctx)
+{
+    const int P = ctx->sp.nphases, G = ctx->G;
+    bool any = false;
+    for (int q = 0; q < P * P; q++) any |= ctx->sp.emodel[q] == 2;
+    if (!any || !ctx->pair_energy_dirty) return OPGPU_OK;
+    if (ctx->sp.pair_mode == OPGPU_PAIRS_HASH)
+        return fail(ctx, OPGPU_E_INVALID, "DISORIENTATION energies are tabulated per grain pair: not with opgpu_set_pair_hash");
+    if (G > kMaxPairTableGrains)
+        return fail(ctx, OPGPU_E_INVALID, "DISORIENTATION energies: at most 16384 grains");
+    const size_t GG = (size_t)G * G;
+    std::vector<double> tab(GG);
+    const double unit[4] = {1.0, 0.0, 0.0, 0.0};
+#pragma omp parallel for
+    for (int a = 0; a < G; a++)
+        for (int b = 0; b < G; b++)
+        {
+            const int q = ctx->h_gphase[a] * P + ctx->h_gphase[b];
+            double v;
+            if (ctx->sp.emodel[q] == 2)
+                v = a == b ? 0.0
+                           : disorientation_energy(ctx->h_quat.empty() ? unit : &ctx->h_quat[4 * (size_t)a],
+                                                   ctx->h_quat.empty() ? unit : &ctx->h_quat[4 * (size_t)b]);
+            else
+                v = ctx->h_user_sigma.empty() ? ctx->sp.sigma_p[q] : ctx->h_user_sigma[(size_t)a * G + b];
+            tab[(size_t)a * G + b] = v;
+        }
+    if (!ctx->d_pair_sigma) CK(dalloc(&ctx->d_pair_sigma, GG));
+    CK(cudaMemcpy(ctx->d_pair_sigma, tab.data(), GG * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->sp.pair_mode = OPGPU_PAIRS_TABLE;
+    ctx->pair_energy_dirty = false;
     return OPGPU_OK;
 }
 
@@ -819,6 +917,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
     if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_step: call opgpu_finalize_initialization first")) return r;
     if (nsteps < 0 || !(dt > 0.0)) return fail(ctx, OPGPU_E_INVALID, "opgpu_step: dt > 0 and nsteps >= 0 required");
     if (ctx->sp.use_dg && !ctx->d_dg) return fail(ctx, OPGPU_E_STATE, "opgpu_step: driving force enabled without values");
+    if (uint32_t r = refresh_pair_energy(ctx)) return r;
     StepParams sp = ctx->sp;
     sp.dt = dt;
     const bool pair_table = sp.use_dg && ctx->G <= kMaxPairTableGrains;
@@ -1163,6 +1262,7 @@ uint32_t copy_grains(opgpu_ctx* ctx, double* vol, double* mx, double* vr, int8_t
 // Fill the G*G driving-force table if it is out of date (the forward step does the same).
 uint32_t refresh_dg_pair(opgpu_ctx* ctx)
 {
+    if (uint32_t r = refresh_pair_energy(ctx)) return r;
     if (ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && ctx->dg_pair_dirty)
     {
         if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, (size_t)ctx->G * ctx->G));

@@ -167,6 +167,20 @@ def nuclei(nx: int, ny: int, nz: int, ngrains: int, seed: int, radius: float, iw
     return counts, idx, val
 
 
+def small_rotations(ngrains: int, seed: int, spread: float) -> np.ndarray:
+    """Unit quaternions (s, x, y, z) of rotations by an angle uniform in [0, spread) about axes
+    uniform on the sphere: orientations whose pairwise disorientations are mostly small."""
+    q = np.empty((ngrains, 4))
+    for g in range(ngrains):
+        u1, u2, u3 = (uniform(seed, STREAM_ORIENTATION, g, k) for k in range(3))
+        cz = 2.0 * u1 - 1.0
+        r = np.sqrt(max(0.0, 1.0 - cz * cz))
+        axis = (r * np.cos(2 * np.pi * u2), r * np.sin(2 * np.pi * u2), cz)
+        half = 0.5 * spread * u3
+        q[g] = (np.cos(half), axis[0] * np.sin(half), axis[1] * np.sin(half), axis[2] * np.sin(half))
+    return q
+
+
 def quaternions(ngrains: int, seed: int) -> np.ndarray:
     """Uniform random unit quaternions (s, x, y, z) per grain by Shoemake's method (Graphics Gems
     III, 1992): u1, u2, u3 uniform; q = (sqrt(1-u1) sin 2pi u2, sqrt(1-u1) cos 2pi u2,

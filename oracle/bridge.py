@@ -193,7 +193,9 @@ def _case_text(case, workdir: Path, dump_steps, threads):
         for b in range(a, P):
             lines += [f"sigma {a} {b} {float(sig[a, b])!r}", f"mu {a} {b} {float(mu[a, b])!r}",
                       f"limit {a} {b} {float(lim[a, b])!r}"]
-            if eps is not None and eps[a, b] != 0.0:
+            if case.disorientation:
+                lines.append(f"energy_model {a} {b} DISORIENTATION")
+            elif eps is not None and eps[a, b] != 0.0:
                 lines += [f"energy_model {a} {b} CUBIC", f"cubic_eps {a} {b} {float(eps[a, b])!r}"]
     if P > 1:
         f = workdir / "grain_phase.bin"

@@ -35,6 +35,7 @@ struct op_sim {
     int* energy_model;            /* [P*P] OP_ENERGY_*                                           */
     double* cubic_eps;            /* [P*P]                                                       */
     double* rot;                  /* [G*9] grain RotationMatrix, row-major                       */
+    double* quat;                 /* [G*4] grain Orientation (s, x, y, z) as given               */
     int aniso;                    /* some phase pair uses an anisotropic energy model            */
     long n;
     int cap;
@@ -154,6 +155,14 @@ op_sim* op_create(const op_params* p, int cap)
      * orientation, normalised as Quaternion::normalized (include/Containers/Quaternion.h:304-311);
      * unit rotation without orientations. */
     s->rot = (double*)calloc((size_t)G*9, sizeof(double));
+    s->quat = (double*)malloc((size_t)G*4*sizeof(double));
+    for (int g = 0; g < G; g++)
+    {
+        s->quat[4*g]     = p->quat ? p->quat[4*g]     : 1.0;
+        s->quat[4*g + 1] = p->quat ? p->quat[4*g + 1] : 0.0;
+        s->quat[4*g + 2] = p->quat ? p->quat[4*g + 2] : 0.0;
+        s->quat[4*g + 3] = p->quat ? p->quat[4*g + 3] : 0.0;
+    }
     for (int g = 0; g < G; g++)
     {
         double* R = s->rot + 9*g;
@@ -214,7 +223,7 @@ void op_destroy(op_sim* s)
     free(s->grain_phase); free(s->phase_solid);
     free(s->sigma_phase); free(s->mu_phase); free(s->limit_phase);
     free(s->pair_sigma); free(s->pair_mu); free(s->dg);
-    free(s->energy_model); free(s->cubic_eps); free(s->rot);
+    free(s->energy_model); free(s->cubic_eps); free(s->rot); free(s->quat);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
     free(s->exist); free(s->stage);
@@ -269,9 +278,13 @@ static double ip_mobility(const op_sim* s, int ga, int gb)
     const int P = s->p.nphases;
     return s->mu_phase[s->grain_phase[ga]*P + s->grain_phase[gb]];
 }
+/* InterfaceEnergyModel::Energy of a phase pair; the DISORIENTATION model reads no $Sigma and keeps
+ * the constructor's 0 (include/InterfaceProperties/InterfaceEnergyModel.h:63-70, 303-306). */
 static double phase_energy(const op_sim* s, int pa, int pb)
 {
-    return s->sigma_phase[pa*s->p.nphases + pb];
+    const int q = pa*s->p.nphases + pb;
+    if (s->energy_model[q] == OP_ENERGY_DISORIENTATION) return 0.0;
+    return s->sigma_phase[q];
 }
 
 /* InterfaceEnergyModel::MaxEnergy of a phase pair: Energy for ISO (ReadInputIso), Energy*(1 +
@@ -280,7 +293,55 @@ static double phase_max_energy(const op_sim* s, int pa, int pb)
 {
     const int q = pa*s->p.nphases + pb;
     if (s->energy_model[q] == OP_ENERGY_CUBIC) return s->sigma_phase[q]*(1.0 + s->cubic_eps[q]*1.41);
+    if (s->energy_model[q] == OP_ENERGY_DISORIENTATION) return 0.0;   /* MaxEnergy keeps its 0 */
     return s->sigma_phase[q];
+}
+
+/* Tools::getDisorientationCubic (src/Tools.cpp:626-678): the rotation angle 2*acos(max |c|) of
+ * dQ = A * B.inverted() over the 24 combinations c of its components (Grimmer 1974), with the
+ * reference's factors 0.707 and 0.5.  Quaternion product and inverse as
+ * include/Containers/Quaternion.h:257-266, 313-339 (component 0 = s). */
+static double disorientation_cubic(const double* A, const double* B)
+{
+    const double bs = B[0], bx = B[1], by = B[2], bz = B[3];
+    const double n2 = bs*bs + (bx*bx + by*by + bz*bz);
+    const double is = bs/n2, ix = (bx*(-1.0))/n2, iy = (by*(-1.0))/n2, iz = (bz*(-1.0))/n2;
+    const double as = A[0], ax = A[1], ay = A[2], az = A[3];
+    double d[4];
+    d[1] =  ax*is + ay*iz - az*iy + as*ix;
+    d[2] = -ax*iz + ay*is + az*ix + as*iy;
+    d[3] =  ax*iy - ay*ix + az*is + as*iz;
+    d[0] = -ax*ix - ay*iy - az*iz + as*is;
+    double c[24];
+    c[0] = d[0]; c[1] = d[1]; c[2] = d[2]; c[3] = d[3];
+    c[4]  = (d[0] + d[1])*0.707; c[5]  = (d[0] - d[1])*0.707;
+    c[6]  = (d[2] + d[3])*0.707; c[7]  = (d[2] - d[3])*0.707;
+    c[8]  = (d[0] + d[2])*0.707; c[9]  = (d[0] - d[2])*0.707;
+    c[10] = (d[1] + d[3])*0.707; c[11] = (d[1] - d[3])*0.707;
+    c[12] = (d[0] + d[3])*0.707; c[13] = (d[0] - d[3])*0.707;
+    c[14] = (d[1] + d[2])*0.707; c[15] = (d[1] - d[2])*0.707;
+    c[16] = (d[0] + d[1] + d[2] + d[3])*0.5;
+    c[17] = (d[0] + d[1] - d[2] - d[3])*0.5;
+    c[18] = (d[0] - d[1] + d[2] - d[3])*0.5;
+    c[19] = (d[0] - d[1] - d[2] + d[3])*0.5;
+    c[20] = (d[0] + d[1] + d[2] - d[3])*0.5;
+    c[21] = (d[0] + d[1] - d[2] + d[3])*0.5;
+    c[22] = (d[0] - d[1] + d[2] + d[3])*0.5;
+    c[23] = (d[0] - d[1] - d[2] - d[3])*0.5;
+    double m = 0.0;
+    for (int k = 0; k < 24; k++)
+        if (m < fabs(c[k])) m = fabs(c[k]);
+    return 2*acos(m);
+}
+
+/* InterfaceEnergyModel::CalculateDisorientation (InterfaceEnergyModel.h:308-323): a
+ * Read-Shockley-type energy of the disorientation angle, constant above 0.349066 rad. */
+static double disorientation_energy(const double* A, const double* B)
+{
+    const double constant = 0.85;
+    const double mis = disorientation_cubic(A, B);
+    if (mis <= 0.349066) return mis*constant*(0.8 - log(mis));
+    return 0.349066*constant*(0.8 - log(0.349066));
 }
 
 /* InterfaceOrientation (src/InterfaceProperties.cpp:39-45): the normal -grad(phi) normalised
@@ -324,6 +385,8 @@ static double voxel_energy(const op_sim* s, const entry* L, int a, int b)
     const int pA = s->grain_phase[ga], pB = s->grain_phase[gb];
     const int q = pA*s->p.nphases + pB;
     if (s->energy_model[q] == OP_ENERGY_ISO) return ip_energy(s, ga, gb);
+    if (s->energy_model[q] == OP_ENERGY_DISORIENTATION)   /* InterfaceProperties.cpp:629-634 */
+        return disorientation_energy(s->quat + 4*ga, s->quat + 4*gb);
     double loc = 0.0, wA = 0.0, wB = 0.0;
     if (s->phase_solid[pA])
     {
@@ -395,7 +458,11 @@ static int do_increments(const op_sim* s, const entry* L, int n, pair* P)
         if (c != a && c != b)
         {
             const int gc = L[c].idx;
-            dPhi_dt += (s->aniso ? voxel_energy(s, L, b, c) - voxel_energy(s, L, a, c)
+            /* IP.Properties holds one energy per grain pair, evaluated by SetSR with the pair's
+             * earlier list entry first (InterfaceProperties.cpp:609-614): an order-dependent model
+             * is evaluated here in that order too */
+            dPhi_dt += (s->aniso ? voxel_energy(s, L, b < c ? b : c, b < c ? c : b)
+                                   - voxel_energy(s, L, a < c ? a : c, a < c ? c : a)
                                  : ip_energy(s, gb, gc) - ip_energy(s, ga, gc))
                       *(L[c].lap + 0.5*(1.0 + scale)*Prefactor*L[c].val);
             /* TripleJunctionModels::Model (:536-552) */

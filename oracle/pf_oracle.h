@@ -19,7 +19,7 @@ extern "C" {
 
 enum { OP_STENCIL_SIMPLE = 0, OP_STENCIL_ISOTROPIC = 1, OP_STENCIL_LB = 2 };
 enum { OP_STAGE_STABLE = 0, OP_STAGE_SEED = 1, OP_STAGE_NUCLEUS = 2 };
-enum { OP_ENERGY_ISO = 0, OP_ENERGY_CUBIC = 1 };
+enum { OP_ENERGY_ISO = 0, OP_ENERGY_CUBIC = 1, OP_ENERGY_DISORIENTATION = 2 };
 
 /* Status bits reported by op_step (OR-ed over all voxels and steps since the last call). */
 enum {

@@ -37,6 +37,11 @@ GOLDEN_CASES = {
                              phase_solid=(0, 1), phase_cubic_eps=((0.0, 0.02), (0.02, 0.0)), phase_dg=(0.1, 0.0),
                              init="nuclei", nucleus_radius=4.0, orientations=True, name="cubic_nuclei_24"),
                         [1, 10, 40]),
+    # DISORIENTATION energy model: per-grain-pair energies from the cubic disorientation of
+    # orientations spread over up to 0.6 rad (pairs below and above the 0.349 rad cap)
+    "disorientation_20": (Case(20, 20, 20, 12, seed=11, iwidth=4.0, dt=0.1, orientations=True,
+                               orientation_spread=0.6, disorientation=True, name="disorientation_20"),
+                          [1, 40]),
 }
 
 
