@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define OPGPU_ABI_VERSION 1
+#define OPGPU_ABI_VERSION 2
 
 /* ---- codes --------------------------------------------------------------------------------- */
 #define OPGPU_OK                0u
@@ -79,15 +79,20 @@ typedef struct opgpu_model {
     double  nucleus_volume_factor;   /* default 1.0                                               */
     /* Anisotropic interface energy (InterfaceEnergyModel.h:78-94, 325-345; InterfaceProperties.cpp:
      * 617-673); any may be NULL (all ISO, all phases solid). */
-    const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC, 2 = DISORIENTATION ($EnergyModel_a_b;
+    const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC, 2 = DISORIENTATION, 3 = HEXBOETTGER,
+                                      4 = HEXSUN, 5 = HEXYANG ($EnergyModel_a_b;
                                       DISORIENTATION: InterfaceEnergyModel.h:303-323, the energy of
                                       a grain pair from the cubic disorientation of the two grains'
                                       orientations (opgpu_set_orientations), tabulated per grain pair;
                                       its Energy and MaxEnergy are 0 as in the reference, so with
                                       $Limiting on the driving force of such pairs is limited to 0) */
-    const double* cubic_eps;       /* [P*P] CUBIC strength ($EpsilonE_a_b)                        */
+    const double* cubic_eps;       /* [P*P] Epsilon1 of the CUBIC and HEX* models ($EpsilonE_a_b;
+                                      HEXSUN $EpsilonE20_a_b, HEXYANG $EpsilonE1_a_b)              */
     const int32_t* phase_solid;    /* [P] 1 = Solid, 0 = Liquid ($State_p); anisotropy weights
                                       only count solid grains                                     */
+    const double* model_eps;       /* [P*P*3] Epsilon2..4 of the HEX models (HEXSUN: $EpsilonE40,
+                                      $EpsilonE60, $EpsilonE66; HEXYANG: $EpsilonE2, $EpsilonE3, -;
+                                      InterfaceEnergyModel.h:105-134, 365-399); NULL: zeros       */
 } opgpu_model;
 
 typedef struct opgpu_stats {

@@ -60,7 +60,8 @@ class Model(C.Structure):
                 ("limit", C.POINTER(C.c_double)), ("limiting", C.c_int32), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int32),
                 ("nucleus_volume_factor", C.c_double), ("energy_model", C.POINTER(C.c_int32)),
-                ("cubic_eps", C.POINTER(C.c_double)), ("phase_solid", C.POINTER(C.c_int32))]
+                ("cubic_eps", C.POINTER(C.c_double)), ("phase_solid", C.POINTER(C.c_int32)),
+                ("model_eps", C.POINTER(C.c_double))]
 
 
 class Stats(C.Structure):

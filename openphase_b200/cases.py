@@ -55,6 +55,8 @@ class Case:
     orientations: bool = False                 # random unit quaternion per grain
     orientation_spread: float = 0.0            # > 0: rotations by at most this angle (rad) instead
     disorientation: bool = False               # DISORIENTATION energy model for every phase pair
+    hex_model: str = ""                        # HEXBOETTGER / HEXSUN / HEXYANG in place of CUBIC
+    hex_eps: tuple = (0.0, 0.0, 0.0)           # Epsilon2..4 of the HEX model (Epsilon1: phase_cubic_eps)
 
     @property
     def n(self) -> int:
@@ -84,7 +86,16 @@ class Case:
         if self.disorientation:
             return np.full((self.nphases, self.nphases), 2, dtype=np.int32)
         e = self.cubic_eps()
-        return None if e is None else (e != 0.0).astype(np.int32)
+        if e is None:
+            return None
+        code = {"": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.hex_model]
+        return np.where(e != 0.0, code, 0).astype(np.int32)
+
+    def model_eps(self) -> Optional[np.ndarray]:
+        """P x P x 3: Epsilon2..4 of the HEX models."""
+        if not self.hex_model or self.phase_cubic_eps is None:
+            return None
+        return np.broadcast_to(np.asarray(self.hex_eps, dtype=np.float64), (self.nphases, self.nphases, 3)).copy()
 
     def grain_phase(self) -> np.ndarray:
         g = np.zeros(self.ngrains, dtype=np.int32)

@@ -58,19 +58,21 @@ class Context:
     # ---- parameters
     def set_model(self, sigma, mu, *, limit=None, limiting=True, regularization=1.0, tj_factor=0.0,
                   consider_nucleus_volume=True, nucleus_volume_factor=1.0, energy_model=None, cubic_eps=None,
-                  phase_solid=None):
+                  phase_solid=None, model_eps=None):
         sigma = np.ascontiguousarray(np.atleast_2d(sigma), dtype=np.float64)
         mu = np.ascontiguousarray(np.atleast_2d(mu), dtype=np.float64)
         lim = None if limit is None else np.ascontiguousarray(np.atleast_2d(limit), dtype=np.float64)
         em = None if energy_model is None else np.ascontiguousarray(energy_model, dtype=np.int32)
         eps = None if cubic_eps is None else np.ascontiguousarray(cubic_eps, dtype=np.float64)
         sol = None if phase_solid is None else np.ascontiguousarray(phase_solid, dtype=np.int32)
+        meps = None if model_eps is None else np.ascontiguousarray(model_eps, dtype=np.float64)
         as_ptr = lambda a, t: a.ctypes.data_as(C.POINTER(t)) if a is not None else None  # noqa: E731
         m = Model(nphases=sigma.shape[0], sigma=as_ptr(sigma, C.c_double), mu=as_ptr(mu, C.c_double),
                   limit=as_ptr(lim, C.c_double), limiting=int(limiting), regularization=regularization,
                   tj_factor=tj_factor, consider_nucleus_volume=int(consider_nucleus_volume),
                   nucleus_volume_factor=nucleus_volume_factor, energy_model=as_ptr(em, C.c_int32),
-                  cubic_eps=as_ptr(eps, C.c_double), phase_solid=as_ptr(sol, C.c_int32))
+                  cubic_eps=as_ptr(eps, C.c_double), phase_solid=as_ptr(sol, C.c_int32),
+                  model_eps=as_ptr(meps, C.c_double))
         _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
 
     def set_orientations(self, quat):
@@ -249,7 +251,8 @@ class Context:
                   gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
         ctx.set_model(case.sigma_phase(), case.mu_phase(), limit=case.limit_phase(), limiting=case.limiting,
                       regularization=case.regularization, tj_factor=case.tj_factor,
-                      energy_model=case.energy_models(), cubic_eps=case.cubic_eps(), phase_solid=case.solid_phase())
+                      energy_model=case.energy_models(), cubic_eps=case.cubic_eps(), phase_solid=case.solid_phase(),
+                      model_eps=case.model_eps())
         ctx.set_grains(case.ngrains, phase=case.grain_phase())
         if case.orientations:
             ctx.set_orientations(case.quaternions())

@@ -575,16 +575,18 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         sp.mu_p[q] = m->mu[q];
         const double lim = m->limit ? m->limit[q] : 0.95;   // src/DrivingForce.cpp:161
         const int model = m->energy_model ? m->energy_model[q] : 0;
-        if (model < 0 || model > 2)
-            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO), 1 (CUBIC) or 2 (DISORIENTATION)");
+        if (model < 0 || model > 5)
+            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) .. 5 (HEXYANG)");
         sp.emodel[q] = (signed char)model;
-        sp.eps_p[q] = (model == 1 && m->cubic_eps) ? m->cubic_eps[q] : 0.0;
+        const bool normal_model = model == 1 || model >= 3;
+        sp.eps_p[q] = (normal_model && m->cubic_eps) ? m->cubic_eps[q] : 0.0;
+        for (int k = 0; k < 3; k++) sp.eps_x[q][k] = (model >= 4 && m->model_eps) ? m->model_eps[3 * q + k] : 0.0;
         // DISORIENTATION reads no $Sigma: its Energy and MaxEnergy keep the constructor's 0
         // (InterfaceEnergyModel.h:63-70, 303-306), which the triple-junction term and the
         // driving-force limiter use
         if (model == 2) sp.sigma_p[q] = 0.0;
-        // MaxEnergy: Energy for ISO (InterfaceEnergyModel.h:82), Energy*(1 + Epsilon*1.41) for CUBIC
-        // (ReadInputCubic, InterfaceEnergyModel.h:87-94), 0 for DISORIENTATION
+        // MaxEnergy: Energy for ISO and the HEX models (InterfaceEnergyModel.h:82, 105-134),
+        // Energy*(1 + Epsilon*1.41) for CUBIC (ReadInputCubic, :87-94), 0 for DISORIENTATION
         sp.maxe_p[q] = model == 1 ? m->sigma[q] * (1.0 + sp.eps_p[q] * 1.41) : (model == 2 ? 0.0 : m->sigma[q]);
         // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor
         double allowed = lim * sp.pref_df * sp.maxe_p[q];
@@ -592,7 +594,7 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         sp.allowed_p[q] = allowed;
     }
     sp.aniso = 0;   // models of the interface normal (the disorientation energy depends on the grain pair only)
-    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1;
+    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1 || sp.emodel[q] >= 3;
     for (int a = 0; a < P; a++) sp.solid_p[a] = (signed char)(m->phase_solid ? (m->phase_solid[a] != 0) : 1);
     ctx->nvf = m->nucleus_volume_factor > 0.0 ? m->nucleus_volume_factor : 1.0;
     ctx->model_set = true;

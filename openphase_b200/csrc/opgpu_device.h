@@ -68,11 +68,13 @@ struct StepParams {
     int ngrains;
     int use_dg;
     // anisotropic interface energy (InterfaceProperties::SetSR, src/InterfaceProperties.cpp:617-673):
-    // per phase pair the model (0 ISO, 1 CUBIC), its epsilon and MaxEnergy; per phase solid (1) or
+    // per phase pair the model (0 ISO, 1 CUBIC, 2 DISORIENTATION, 3 HEXBOETTGER, 4 HEXSUN, 5 HEXYANG),
+    // its Epsilon1 (eps_p) and Epsilon2..4 (eps_x) and MaxEnergy; per phase solid (1) or
     // liquid (0); the gradient stencil in GradientStencil::Set order with its weights per axis
     int aniso;
     signed char emodel[kMaxPhases * kMaxPhases];
     double eps_p[kMaxPhases * kMaxPhases];
+    double eps_x[kMaxPhases * kMaxPhases][3];
     double maxe_p[kMaxPhases * kMaxPhases];
     signed char solid_p[kMaxPhases];
     int ngs;

@@ -139,10 +139,37 @@ __device__ __forceinline__ void interface_orientation(const double* g3, const do
     }
 }
 
-// InterfaceEnergyModel::Calculate, CUBIC (include/InterfaceProperties/InterfaceEnergyModel.h:325-345).
-__device__ __forceinline__ double cubic_energy(double energy, double eps, const double* n)
+// InterfaceEnergyModel::Calculate (include/InterfaceProperties/InterfaceEnergyModel.h:325-399) for
+// the models of the interface normal n: CUBIC, HEXBOETTGER (Boettger et al. 2006), HEXSUN (Sun et
+// al. 2006) and HEXYANG (Yang et al. 2015), in the reference's operation order.
+__device__ __forceinline__ double model_energy(const StepParams& p, int q, const double* n)
 {
-    return energy * (1.0 + eps * (1.5 - 2.5 * (pow(n[0], 4.0) + pow(n[1], 4.0) + pow(n[2], 4.0))));
+    const double E = p.sigma_p[q], e1 = p.eps_p[q];
+    const double x = n[0], y = n[1], z = n[2];
+    switch (p.emodel[q])
+    {
+        case 3:
+            return E * (1.0 - e1 * (pow(x, 6.0) - pow(y, 6.0) - 15.0 * pow(x, 4.0) * y * y + 15.0 * pow(y, 4.0) * x * x
+                                    + (5.0 * pow(z, 4.0) - 5.0 * pow(z, 2.0) + pow(z, 6.0))));
+        case 4:
+        {
+            const double pi = 3.14159265358979323846;
+            const double e2 = p.eps_x[q][0], e3 = p.eps_x[q][1], e4 = p.eps_x[q][2];
+            return E * (1.0 + e1 * sqrt(5.0 / 16.0 / pi) * (3.0 * z * z - 1.0)
+                        + e2 * 3.0 / 16.0 / sqrt(pi) * (35.0 * pow(z, 4.0) - 30.0 * z * z + 3.0)
+                        + e3 * sqrt(13.0 / pi) / 32.0 * (231.0 * pow(z, 6.0) - 315.0 * pow(z, 4.0) + 105.0 * z * z - 5.0)
+                        + e4 * sqrt(6006.0 / pi) / 64.0
+                              * (pow(x, 6.0) - 15.0 * pow(x, 4.0) * y * y + 15.0 * x * x * pow(y, 4.0) - pow(y, 6.0)));
+        }
+        case 5:
+        {
+            const double e2 = p.eps_x[q][0], e3 = p.eps_x[q][1];
+            return E * (1.0 + e1 * pow((3.0 * z * z - 1.0), 2.0)
+                        + e2 * pow((x * x * x - 3.0 * x * y * y), 2.0) * pow((9.0 * z * z - 1.0 + e3), 2.0));
+        }
+        default:
+            return E * (1.0 + e1 * (1.5 - 2.5 * (pow(x, 4.0) + pow(y, 4.0) + pow(z, 4.0))));
+    }
 }
 
 // The interface energy of the pair (i, j) of a voxel's list as InterfaceProperties::SetSR stores it
@@ -156,7 +183,7 @@ __device__ __forceinline__ double voxel_energy(const StepParams& p, const StepAr
     const int gi = sc.g[i * S], gj = sc.g[j * S];
     const int pA = a.gphase[gi], pB = a.gphase[gj];
     const int q = pA * p.nphases + pB;
-    if (p.emodel[q] == 0) return pair_energy(p, a, gi, gj);
+    if (p.emodel[q] == 0 || p.emodel[q] == 2) return pair_energy(p, a, gi, gj);   // ISO, per-pair table
     double loc = 0.0, wA = 0.0, wB = 0.0;
     if (p.solid_p[pA])
     {
@@ -167,7 +194,7 @@ __device__ __forceinline__ double voxel_energy(const StepParams& p, const StepAr
             const double g3[3] = {(double)sc.grad[(3 * i) * S], (double)sc.grad[(3 * i + 1) * S], (double)sc.grad[(3 * i + 2) * S]};
             double n[3];
             interface_orientation(g3, a.grot + 9 * (long long)gi, n);
-            loc += cubic_energy(p.sigma_p[q], p.eps_p[q], n) * wA;
+            loc += model_energy(p, q, n) * wA;
         }
         else wA = 0.0;
     }
@@ -180,7 +207,7 @@ __device__ __forceinline__ double voxel_energy(const StepParams& p, const StepAr
             const double g3[3] = {(double)sc.grad[(3 * j) * S], (double)sc.grad[(3 * j + 1) * S], (double)sc.grad[(3 * j + 2) * S]};
             double n[3];
             interface_orientation(g3, a.grot + 9 * (long long)gj, n);
-            loc += cubic_energy(p.sigma_p[q], p.eps_p[q], n) * wB;
+            loc += model_energy(p, q, n) * wB;
         }
         else wB = 0.0;
     }

@@ -29,7 +29,7 @@ class OpParams(C.Structure):
                 ("stencil", C.c_int), ("gradient_stencil", C.c_int), ("nphases", C.c_int), ("ngrains", C.c_int),
                 ("grain_phase", C.c_void_p), ("phase_solid", C.c_void_p), ("sigma_phase", C.c_void_p),
                 ("mu_phase", C.c_void_p), ("energy_model", C.c_void_p), ("cubic_eps", C.c_void_p),
-                ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
+                ("model_eps", C.c_void_p), ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
                 ("limiting", C.c_int), ("limit_phase", C.c_void_p), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int),
                 ("nucleus_volume_factor", C.c_double), ("threads", C.c_int)]
@@ -101,6 +101,8 @@ class Oracle:
         em = keep(em.astype(np.int32)) if em is not None else None
         eps = case.cubic_eps()
         eps = keep(eps) if eps is not None else None
+        meps = case.model_eps()
+        meps = keep(meps) if meps is not None else None
         quat = case.quaternions()
         quat = keep(quat.astype(np.float64)) if quat is not None else None
         ps = case.pair_sigma()
@@ -113,6 +115,7 @@ class Oracle:
                      sigma_phase=_p(sig).value, mu_phase=_p(mu).value,
                      energy_model=_p(em).value if em is not None else None,
                      cubic_eps=_p(eps).value if eps is not None else None,
+                     model_eps=_p(meps).value if meps is not None else None,
                      quat=_p(quat).value if quat is not None else None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
                      dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
                      limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
@@ -196,7 +199,10 @@ def _case_text(case, workdir: Path, dump_steps, threads):
             if case.disorientation:
                 lines.append(f"energy_model {a} {b} DISORIENTATION")
             elif eps is not None and eps[a, b] != 0.0:
-                lines += [f"energy_model {a} {b} CUBIC", f"cubic_eps {a} {b} {float(eps[a, b])!r}"]
+                name = case.hex_model or "CUBIC"
+                lines += [f"energy_model {a} {b} {name}", f"cubic_eps {a} {b} {float(eps[a, b])!r}"]
+                if case.hex_model:
+                    lines.append(f"model_eps {a} {b} " + " ".join(repr(float(e)) for e in case.model_eps()[a, b]))
     if P > 1:
         f = workdir / "grain_phase.bin"
         case.grain_phase().astype(np.int32).tofile(f)

@@ -33,7 +33,8 @@ struct op_sim {
     int* phase_solid;
     double *sigma_phase, *mu_phase, *limit_phase, *pair_sigma, *pair_mu, *dg;
     int* energy_model;            /* [P*P] OP_ENERGY_*                                           */
-    double* cubic_eps;            /* [P*P]                                                       */
+    double* cubic_eps;            /* [P*P] Epsilon1                                              */
+    double* model_eps;            /* [P*P*3] Epsilon2..4                                         */
     double* rot;                  /* [G*9] grain RotationMatrix, row-major                       */
     double* quat;                 /* [G*4] grain Orientation (s, x, y, z) as given               */
     int aniso;                    /* some phase pair uses an anisotropic energy model            */
@@ -144,6 +145,8 @@ op_sim* op_create(const op_params* p, int cap)
     s->p.pair_sigma = s->pair_sigma; s->p.pair_mu = s->pair_mu; s->p.dg = s->dg;
     s->energy_model = (int*)calloc((size_t)P*P, sizeof(int));
     s->cubic_eps = (double*)calloc((size_t)P*P, sizeof(double));
+    s->model_eps = (double*)calloc((size_t)P*P*3, sizeof(double));
+    if (p->model_eps) memcpy(s->model_eps, p->model_eps, (size_t)P*P*3*sizeof(double));
     s->aniso = 0;
     for (int q = 0; q < P*P; q++)
     {
@@ -187,7 +190,8 @@ op_sim* op_create(const op_params* p, int cap)
         R[7] =       2.0*(V1*V2 +  S*V0);
         R[8] = 1.0 - 2.0*(V0*V0 + V1*V1);
     }
-    s->p.energy_model = s->energy_model; s->p.cubic_eps = s->cubic_eps; s->p.quat = NULL;
+    s->p.energy_model = s->energy_model; s->p.cubic_eps = s->cubic_eps; s->p.model_eps = s->model_eps;
+    s->p.quat = NULL;
     if (s->p.nucleus_volume_factor == 0.0) s->p.nucleus_volume_factor = 1.0;
     s->n = (long)p->nx * p->ny * p->nz;
     s->cap = cap;
@@ -223,7 +227,7 @@ void op_destroy(op_sim* s)
     free(s->grain_phase); free(s->phase_solid);
     free(s->sigma_phase); free(s->mu_phase); free(s->limit_phase);
     free(s->pair_sigma); free(s->pair_mu); free(s->dg);
-    free(s->energy_model); free(s->cubic_eps); free(s->rot); free(s->quat);
+    free(s->energy_model); free(s->cubic_eps); free(s->model_eps); free(s->rot); free(s->quat);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
     free(s->exist); free(s->stage);
@@ -369,10 +373,28 @@ static void interface_orientation(const op_sim* s, const entry* e, double out[3]
     }
 }
 
-/* InterfaceEnergyModel::Calculate, CUBIC (InterfaceEnergyModel.h:325-345). */
-static double cubic_energy(double energy, double eps, const double n[3])
+/* InterfaceEnergyModel::Calculate (InterfaceEnergyModel.h:325-399) of the normal n for the phase
+ * pair q: CUBIC, HEXBOETTGER, HEXSUN, HEXYANG, each expression in the reference's operation order. */
+static double model_energy(const op_sim* s, int q, const double n[3])
 {
-    return energy*(1.0 + eps*(1.5 - 2.5*(pow(n[0], 4) + pow(n[1], 4) + pow(n[2], 4))));
+    const double E = s->sigma_phase[q], e1 = s->cubic_eps[q];
+    const double* ex = s->model_eps + 3*q;
+    const double x = n[0], y = n[1], z = n[2];
+    switch (s->energy_model[q])
+    {
+        case OP_ENERGY_HEXBOETTGER:
+            return E*(1.0 - e1*(pow(x, 6) - pow(y, 6) - 15.0*pow(x, 4)*y*y + 15.0*pow(y, 4)*x*x
+                                + (5.0*pow(z, 4) - 5.0*pow(z, 2) + pow(z, 6))));
+        case OP_ENERGY_HEXSUN:
+            return E*(1.0 + e1*sqrt(5.0/16.0/OP_PI)*(3.0*z*z - 1.0)
+                      + ex[0]*3.0/16.0/sqrt(OP_PI)*(35.0*pow(z, 4) - 30.0*z*z + 3.0)
+                      + ex[1]*sqrt(13.0/OP_PI)/32.0*(231.0*pow(z, 6) - 315.0*pow(z, 4) + 105.0*z*z - 5.0)
+                      + ex[2]*sqrt(6006.0/OP_PI)/64.0*(pow(x, 6) - 15.0*pow(x, 4)*y*y + 15.0*x*x*pow(y, 4) - pow(y, 6)));
+        case OP_ENERGY_HEXYANG:
+            return E*(1.0 + e1*pow((3.0*z*z - 1.0), 2) + ex[0]*pow((x*x*x - 3.0*x*y*y), 2)*pow((9.0*z*z - 1.0 + ex[1]), 2));
+        default:   /* CUBIC */
+            return E*(1.0 + e1*(1.5 - 2.5*(pow(x, 4) + pow(y, 4) + pow(z, 4))));
+    }
 }
 
 /* The energy InterfaceProperties::SetSR (src/InterfaceProperties.cpp:617-673) stores for the pair of
@@ -395,7 +417,7 @@ static double voxel_energy(const op_sim* s, const entry* L, int a, int b)
         {
             double n[3];
             interface_orientation(s, &L[a], n);
-            loc += cubic_energy(s->sigma_phase[q], s->cubic_eps[q], n)*wA;
+            loc += model_energy(s, q, n)*wA;
         }
         else wA = 0.0;
     }
@@ -406,7 +428,7 @@ static double voxel_energy(const op_sim* s, const entry* L, int a, int b)
         {
             double n[3];
             interface_orientation(s, &L[b], n);
-            loc += cubic_energy(s->sigma_phase[q], s->cubic_eps[q], n)*wB;
+            loc += model_energy(s, q, n)*wB;
         }
         else wB = 0.0;
     }

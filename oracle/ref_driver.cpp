@@ -57,6 +57,7 @@ struct Case
     std::vector<std::string> phase_state;
     std::vector<double> quat;      // [G*4] grain orientations (s, x, y, z), empty: none
     std::map<std::pair<int,int>, double> sigma, mu, limit, cubic_eps;
+    std::map<std::pair<int,int>, std::vector<double>> model_eps;   // Epsilon2..4 of the HEX models
     std::map<std::pair<int,int>, std::string> energy_model;
     int ngrains = 0;
     std::vector<int> grain_phase;
@@ -118,6 +119,7 @@ static Case parse_case(const std::string& path)
         else if (key == "limit") { int a, b; double v; is >> a >> b >> v; c.limit[{a,b}] = v; }
         else if (key == "energy_model") { int a, b; std::string m; is >> a >> b >> m; c.energy_model[{a,b}] = m; }
         else if (key == "cubic_eps") { int a, b; double v; is >> a >> b >> v; c.cubic_eps[{a,b}] = v; }
+        else if (key == "model_eps") { int a, b; double e2, e3, e4; is >> a >> b >> e2 >> e3 >> e4; c.model_eps[{a,b}] = {e2, e3, e4}; }
         else if (key == "ngrains") is >> c.ngrains;
         else if (key == "grain_phase_file") is >> grain_phase_file;
         else if (key == "pair_sigma_file") is >> pair_sigma_file;
@@ -171,11 +173,16 @@ static void write_opi(const Case& c, const std::string& path)
         double m = c.mu.count({a,b}) ? c.mu.at({a,b}) : 1.0;
         o << "$EnergyModel_" << a << "_" << b << " : " << model << "\n";
         o << "$Sigma_" << a << "_" << b << " : " << s << "\n";
-        if (model == "CUBIC")
-        {
-            double e = c.cubic_eps.count({a,b}) ? c.cubic_eps.at({a,b}) : 0.0;
-            o << "$EpsilonE_" << a << "_" << b << " : " << e << "\n";
-        }
+        const double e1 = c.cubic_eps.count({a,b}) ? c.cubic_eps.at({a,b}) : 0.0;
+        const std::vector<double> ex = c.model_eps.count({a,b}) ? c.model_eps.at({a,b}) : std::vector<double>(3, 0.0);
+        const std::string ab = std::to_string(a) + "_" + std::to_string(b);
+        if (model == "CUBIC" or model == "HEXBOETTGER") o << "$EpsilonE_" << ab << " : " << e1 << "\n";
+        if (model == "HEXSUN")
+            o << "$EpsilonE20_" << ab << " : " << e1 << "\n" << "$EpsilonE40_" << ab << " : " << ex[0] << "\n"
+              << "$EpsilonE60_" << ab << " : " << ex[1] << "\n" << "$EpsilonE66_" << ab << " : " << ex[2] << "\n";
+        if (model == "HEXYANG")
+            o << "$EpsilonE1_" << ab << " : " << e1 << "\n" << "$EpsilonE2_" << ab << " : " << ex[0] << "\n"
+              << "$EpsilonE3_" << ab << " : " << ex[1] << "\n";
         o << "$MobilityModel_" << a << "_" << b << " : ISO\n";
         o << "$Mu_" << a << "_" << b << " : " << m << "\n";
     }

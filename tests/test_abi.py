@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version_and_device_query():
-    assert lib().opgpu_abi_version() == 1
+    assert lib().opgpu_abi_version() == 2
     assert lib().opgpu_device_count() >= 0
 
 

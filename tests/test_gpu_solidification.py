@@ -48,6 +48,36 @@ def test_fp64_cubic_nuclei_match_oracle(n, grains, checkpoints):
         assert vol <= 1e-10
 
 
+@pytest.mark.parametrize("name", ["cubic_nuclei_24", "hexboettger_nuclei_24", "hexsun_nuclei_24",
+                                  "hexyang_nuclei_24"])
+def test_fp64_energy_models_match_oracle_and_reference(name):
+    """CUBIC and the hexagonal models (HEXBOETTGER, HEXSUN, HEXYANG; InterfaceEnergyModel.h:325-399)
+    on the solid-liquid pairs: the FP64 form against the oracle over 100 steps and against the
+    reference's own states (tests/golden/<name>.npz) at its checkpoints."""
+    from tests.golden.make_golden import GOLDEN_CASES
+    from pathlib import Path
+    case, golden_steps = GOLDEN_CASES[name]
+    z = np.load(Path(__file__).resolve().parent / "golden" / f"{name}.npz")
+    state = case.initial_state()
+    ora = Oracle(case, *state)
+    ctx = Context.from_case(case, precision="fp64", k_slots=16, state=state)
+    prev = 0
+    for s in sorted(set(golden_steps) | {100}):
+        assert ctx.step(case.dt, s - prev) & 0b11 == 0
+        ora.step(s - prev)
+        prev = s
+        mine = ctx.download()
+        r = compare_states(mine, ora.state(positive_only=True), case.ngrains)
+        assert r["non_borderline_mismatch_voxels"] == 0 and r["max_dphi"] <= 1e-9, (s, r)
+        if f"s{s}_val" in z:
+            c, i, v = z[f"s{s}_counts"].astype(np.int64), z[f"s{s}_idx"].astype(np.int32), z[f"s{s}_val"]
+            keep = v > 0.0
+            ref = (np.bincount(np.repeat(np.arange(c.size), c)[keep], minlength=c.size).astype(np.int32),
+                   i[keep], v[keep])
+            r = compare_states(mine, ref, case.ngrains)
+            assert r["non_borderline_mismatch_voxels"] == 0 and r["max_dphi"] <= 1e-9, (s, r)
+
+
 def test_fp32_cubic_nuclei_error_against_fp64_oracle():
     case = _case(40, 17)
     state = case.initial_state()
