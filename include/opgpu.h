@@ -217,13 +217,18 @@ uint32_t opgpu_checkpoint_reserve(opgpu_ctx* ctx, int32_t nslots);
 /* Copy the current state and grain records into / out of a checkpoint slot. */
 uint32_t opgpu_checkpoint_save(opgpu_ctx* ctx, int32_t slot);
 uint32_t opgpu_checkpoint_load(opgpu_ctx* ctx, int32_t slot);
+/* One step (opgpu_step with nsteps = 1) that leaves the state it started from, with its grain
+ * records, in checkpoint `slot`: opgpu_checkpoint_save(slot) + opgpu_step without copying the state
+ * (the slot takes the input buffers; its old buffers become the step's scratch). */
+uint32_t opgpu_step_save_input(opgpu_ctx* ctx, double dt, int32_t slot);
 /* Start a reverse sweep at the current state: the adjoint of every stored value is dL_dV[grain]
  * (dL_dV[G]); the gradient accumulators are zeroed. */
 uint32_t opgpu_adjoint_begin(opgpu_ctx* ctx, const double* dL_dV);
 /* One step backwards.  `slot` holds the state from which one forward step of length dt produced the
  * current state.  Accumulates the parameter gradients of that step, turns the adjoint into that of
- * the slot's state and makes the slot's state current.  OPGPU_E_* bit 6 is raised when the
- * recomputed step does not reproduce the current state's lists. */
+ * the slot's state and makes the slot's state current: the slot and the current state exchange
+ * their buffers, so that afterwards the slot holds the state that was current.  OPGPU_E_* bit 6 is
+ * raised when the recomputed step does not reproduce the current state's lists. */
 uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt);
 /* Accumulated gradients: dL_dsigma[G*G], dL_dmu[G*G] (symmetric, zero diagonal), dL_ddG[G]; any may
  * be NULL. */

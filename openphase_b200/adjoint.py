@@ -70,8 +70,7 @@ class Rollout:
             t1 = min(self.T, t0 + self.C)
             ctx.checkpoint_load(self.seg0 + seg)
             for t in range(t0, t1):
-                ctx.checkpoint_save(self.buf0 + (t - t0))
-                ctx.step(self.dt, 1)
+                ctx.step_save_input(self.dt, self.buf0 + (t - t0))
             for t in range(t1 - 1, t0 - 1, -1):
                 status |= ctx.adjoint_step(self.buf0 + (t - t0), self.dt)
         self.adjoint_status = status

@@ -190,6 +190,10 @@ class Context:
     def checkpoint_save(self, slot: int):
         _check(lib().opgpu_checkpoint_save(self.h, int(slot)), self.h, "checkpoint_save")
 
+    def step_save_input(self, dt, slot: int) -> int:
+        """One step that leaves the state it started from in checkpoint `slot` (no state copy)."""
+        return _check(lib().opgpu_step_save_input(self.h, dt, slot), self.h, "step_save_input")
+
     def checkpoint_load(self, slot: int):
         _check(lib().opgpu_checkpoint_load(self.h, int(slot)), self.h, "checkpoint_load")
 

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 using namespace opgpu;
@@ -1348,6 +1349,24 @@ extern "C" uint32_t opgpu_checkpoint_save(opgpu_ctx* ctx, int32_t slot)
                        ctx->d_exist, ctx->d_gstage);
 }
 
+extern "C" uint32_t opgpu_step_save_input(opgpu_ctx* ctx, double dt, int32_t slot)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_step_save_input: not initialized")) return r;
+    if (slot < 0 || slot >= (int)ctx->slots.size()) return fail(ctx, OPGPU_E_INVALID, "opgpu_step_save_input: no such slot");
+    auto& s = ctx->slots[slot];
+    // the grain records are updated in place by the step: copy them first (G values)
+    if (uint32_t r = copy_grains(ctx, s.volume, s.maxvol, s.vr, s.exist, s.stage, ctx->d_volume, ctx->d_maxvol,
+                                 ctx->d_vr, ctx->d_exist, ctx->d_gstage)) return r;
+    const int in = ctx->cur;
+    if (uint32_t r = enqueue_steps(ctx, dt, 1)) return r;
+    // the step read buffer `in` and wrote the other one: the input state moves into the slot, the
+    // slot's old buffers become the spare state buffer (every step rewrites it)
+    std::swap(ctx->cnt[in], s.cnt);
+    std::swap(ctx->idx[in], s.idx);
+    std::swap(ctx->val[in], s.val);
+    return opgpu_sync(ctx);
+}
+
 extern "C" uint32_t opgpu_checkpoint_load(opgpu_ctx* ctx, int32_t slot)
 {
     if (uint32_t r = require(ctx, ctx && ctx->initialized, "opgpu_checkpoint_load: not initialized")) return r;
@@ -1412,10 +1431,16 @@ extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
         return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: launch");
     ctx->kernel_launches += 12;
     ctx->lam_cur = 1 - ctx->lam_cur;
-    // the state before the step becomes the current state (the adjoint is aligned with it)
-    if (uint32_t r = copy_state(ctx, ctx->cnt[ctx->cur], ctx->idx[ctx->cur], ctx->val[ctx->cur], s.cnt, s.idx, s.val)) return r;
-    if (uint32_t r = copy_grains(ctx, ctx->d_volume, ctx->d_maxvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage,
-                                 s.volume, s.maxvol, s.vr, s.exist, s.stage)) return r;
+    // the state before the step becomes the current state (the adjoint is aligned with it): the slot
+    // and the current state exchange their buffers (same sizes), so no state is copied
+    std::swap(ctx->cnt[ctx->cur], s.cnt);
+    std::swap(ctx->idx[ctx->cur], s.idx);
+    std::swap(ctx->val[ctx->cur], s.val);
+    std::swap(ctx->d_volume, s.volume);
+    std::swap(ctx->d_maxvol, s.maxvol);
+    std::swap(ctx->d_vr, s.vr);
+    std::swap(ctx->d_exist, s.exist);
+    std::swap(ctx->d_gstage, s.stage);
     const uint32_t st = read_status(ctx);
     if (st & OPGPU_E_CUDA) return st;
     return st & OPGPU_SOFT_MASK;

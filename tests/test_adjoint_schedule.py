@@ -32,6 +32,10 @@ class Recorder:
         self.t += n
         return 0
 
+    def step_save_input(self, dt, k):
+        self.checkpoint_save(k)
+        return self.step(dt, 1)
+
     def stats(self):
         return {"entries_out_total": 0}
 
@@ -45,7 +49,8 @@ class Recorder:
         # the adjoint is aligned with the current state, which must be one step after the slot's
         assert self.lam_at == self.t and self.slots[k] == self.t - 1
         self.reverse.append(self.slots[k])
-        self.t = self.slots[k]
+        # the slot and the current state exchange their buffers
+        self.t, self.slots[k] = self.slots[k], self.t
         self.lam_at = self.t
         return 0
 
