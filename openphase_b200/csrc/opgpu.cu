@@ -960,6 +960,9 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
                 }
             }
             CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used], ctx->stream));
+            // "after classify" is recorded at the start too; the tiled path records it again after
+            // its classify kernel (paths without a classify phase leave it at the start)
+            CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used + 1], ctx->stream));
             info.after_classify = ctx->ev_pool[3 * ctx->ev_used + 1];
         }
         const int rc = ctx->fp32 ? launch_step_f32(sp, a, ctx->K, ctx->variant, ctx->stream, &info)
@@ -967,9 +970,6 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
         if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("step launch: ") + cudaGetErrorString((cudaError_t)rc));
         if (ctx->timing)
         {
-            // the generic variant has no classify phase: its "after classify" event is the start
-            if (ctx->variant == kVariantGeneric)
-                CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used + 1], ctx->stream));
             CK(cudaEventRecord(ctx->ev_pool[3 * ctx->ev_used + 2], ctx->stream));
             ctx->ev_used++;
         }

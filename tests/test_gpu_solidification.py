@@ -106,3 +106,20 @@ def test_adjoint_refuses_anisotropic_energies():
         ctx.adjoint_begin(np.zeros(case.ngrains))
     with pytest.raises(OpgpuError):
         ctx.tlm_begin()
+
+
+@pytest.mark.parametrize("aniso", [True, False])
+def test_step_timing_on_every_path(aniso):
+    """opgpu_set_timing on the per-voxel path of anisotropic energies (no classify phase) and on the
+    tiled path: every timed step is counted and the classify share lies within the step."""
+    case = _case(24, 7) if aniso else Case(24, 24, 24, 10, seed=3, iwidth=5.0, dt=0.1, name="iso_24")
+    ctx = Context.from_case(case, precision="fp64", k_slots=16)
+    ctx.step(case.dt, 2)
+    ctx.set_timing(True)
+    ctx.step(case.dt, 3)
+    s = ctx.stats()
+    assert s["timed_launches"] == 3
+    assert s["timed_kernel_ms"] > 0.0
+    assert 0.0 <= s["timed_classify_ms"] <= s["timed_kernel_ms"]
+    if aniso:
+        assert s["timed_classify_ms"] < 0.1 * s["timed_kernel_ms"]
