@@ -80,7 +80,7 @@ typedef struct opgpu_model {
     /* Anisotropic interface energy (InterfaceEnergyModel.h:78-94, 325-345; InterfaceProperties.cpp:
      * 617-673); any may be NULL (all ISO, all phases solid). */
     const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC, 2 = DISORIENTATION, 3 = HEXBOETTGER,
-                                      4 = HEXSUN, 5 = HEXYANG ($EnergyModel_a_b;
+                                      4 = HEXSUN, 5 = HEXYANG, 6 = FACETED ($EnergyModel_a_b;
                                       DISORIENTATION: InterfaceEnergyModel.h:303-323, the energy of
                                       a grain pair from the cubic disorientation of the two grains'
                                       orientations (opgpu_set_orientations), tabulated per grain pair;
@@ -93,6 +93,14 @@ typedef struct opgpu_model {
     const double* model_eps;       /* [P*P*3] Epsilon2..4 of the HEX models (HEXSUN: $EpsilonE40,
                                       $EpsilonE60, $EpsilonE66; HEXYANG: $EpsilonE2, $EpsilonE3, -;
                                       InterfaceEnergyModel.h:105-134, 365-399); NULL: zeros       */
+    /* FACETED (InterfaceEnergyModel.h:196-246, 417-438): the facets of phase pair q are entries
+     * facet_start[q] .. facet_start[q+1]-1 of facet_data, 5 doubles each: h, k, l ($Facet_a_b_n),
+     * SigmaF ($SigmaF_a_b_n), EpsilonEF ($EpsilonEF_a_b_n); facet_family[q] = 1 makes every facet
+     * stand for its family of index permutations ($NfacetFamilies_a_b), 0 for itself ($Nfacets_a_b).
+     * Energy = mean SigmaF, MaxEnergy = max SigmaF.  All three may be NULL without FACETED pairs. */
+    const int32_t* facet_start;    /* [P*P+1]                                                      */
+    const double* facet_data;      /* [facet_start[P*P]*5]                                         */
+    const int32_t* facet_family;   /* [P*P]                                                        */
 } opgpu_model;
 
 typedef struct opgpu_stats {

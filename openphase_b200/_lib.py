@@ -61,7 +61,8 @@ class Model(C.Structure):
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int32),
                 ("nucleus_volume_factor", C.c_double), ("energy_model", C.POINTER(C.c_int32)),
                 ("cubic_eps", C.POINTER(C.c_double)), ("phase_solid", C.POINTER(C.c_int32)),
-                ("model_eps", C.POINTER(C.c_double))]
+                ("model_eps", C.POINTER(C.c_double)), ("facet_start", C.POINTER(C.c_int32)),
+                ("facet_data", C.POINTER(C.c_double)), ("facet_family", C.POINTER(C.c_int32))]
 
 
 class Stats(C.Structure):

@@ -57,6 +57,8 @@ class Case:
     disorientation: bool = False               # DISORIENTATION energy model for every phase pair
     hex_model: str = ""                        # HEXBOETTGER / HEXSUN / HEXYANG in place of CUBIC
     hex_eps: tuple = (0.0, 0.0, 0.0)           # Epsilon2..4 of the HEX model (Epsilon1: phase_cubic_eps)
+    facets: tuple = ()                         # FACETED in place of CUBIC: (h, k, l, SigmaF, EpsilonEF) each
+    facet_families: bool = True                # every facet stands for its family of permutations
 
     @property
     def n(self) -> int:
@@ -88,8 +90,22 @@ class Case:
         e = self.cubic_eps()
         if e is None:
             return None
-        code = {"": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.hex_model]
+        code = 6 if self.facets else {"": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.hex_model]
         return np.where(e != 0.0, code, 0).astype(np.int32)
+
+    def facet_tables(self):
+        """(facet_start[P*P+1], facet_data[F, 5], facet_family[P*P]) for the FACETED pairs, or None."""
+        em = self.energy_models()
+        if not self.facets or em is None:
+            return None
+        P = self.nphases
+        start, rows = [0], []
+        for q in range(P * P):
+            if em.flat[q] == 6:
+                rows += [list(f) for f in self.facets]
+            start.append(len(rows))
+        fam = np.full(P * P, int(self.facet_families), dtype=np.int32)
+        return np.array(start, dtype=np.int32), np.array(rows, dtype=np.float64).reshape(-1, 5), fam
 
     def model_eps(self) -> Optional[np.ndarray]:
         """P x P x 3: Epsilon2..4 of the HEX models."""

@@ -58,7 +58,8 @@ class Context:
     # ---- parameters
     def set_model(self, sigma, mu, *, limit=None, limiting=True, regularization=1.0, tj_factor=0.0,
                   consider_nucleus_volume=True, nucleus_volume_factor=1.0, energy_model=None, cubic_eps=None,
-                  phase_solid=None, model_eps=None):
+                  phase_solid=None, model_eps=None, facets=None):
+        """facets: (facet_start[P*P+1], facet_data[F, 5], facet_family[P*P]) of the FACETED pairs."""
         sigma = np.ascontiguousarray(np.atleast_2d(sigma), dtype=np.float64)
         mu = np.ascontiguousarray(np.atleast_2d(mu), dtype=np.float64)
         lim = None if limit is None else np.ascontiguousarray(np.atleast_2d(limit), dtype=np.float64)
@@ -66,13 +67,17 @@ class Context:
         eps = None if cubic_eps is None else np.ascontiguousarray(cubic_eps, dtype=np.float64)
         sol = None if phase_solid is None else np.ascontiguousarray(phase_solid, dtype=np.int32)
         meps = None if model_eps is None else np.ascontiguousarray(model_eps, dtype=np.float64)
+        fs, fd, ff = (None, None, None) if facets is None else (
+            np.ascontiguousarray(facets[0], dtype=np.int32), np.ascontiguousarray(facets[1], dtype=np.float64),
+            np.ascontiguousarray(facets[2], dtype=np.int32))
         as_ptr = lambda a, t: a.ctypes.data_as(C.POINTER(t)) if a is not None else None  # noqa: E731
         m = Model(nphases=sigma.shape[0], sigma=as_ptr(sigma, C.c_double), mu=as_ptr(mu, C.c_double),
                   limit=as_ptr(lim, C.c_double), limiting=int(limiting), regularization=regularization,
                   tj_factor=tj_factor, consider_nucleus_volume=int(consider_nucleus_volume),
                   nucleus_volume_factor=nucleus_volume_factor, energy_model=as_ptr(em, C.c_int32),
                   cubic_eps=as_ptr(eps, C.c_double), phase_solid=as_ptr(sol, C.c_int32),
-                  model_eps=as_ptr(meps, C.c_double))
+                  model_eps=as_ptr(meps, C.c_double), facet_start=as_ptr(fs, C.c_int32),
+                  facet_data=as_ptr(fd, C.c_double), facet_family=as_ptr(ff, C.c_int32))
         _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
 
     def set_orientations(self, quat):
@@ -256,7 +261,7 @@ class Context:
         ctx.set_model(case.sigma_phase(), case.mu_phase(), limit=case.limit_phase(), limiting=case.limiting,
                       regularization=case.regularization, tj_factor=case.tj_factor,
                       energy_model=case.energy_models(), cubic_eps=case.cubic_eps(), phase_solid=case.solid_phase(),
-                      model_eps=case.model_eps())
+                      model_eps=case.model_eps(), facets=case.facet_tables())
         ctx.set_grains(case.ngrains, phase=case.grain_phase())
         if case.orientations:
             ctx.set_orientations(case.quaternions())

@@ -9,6 +9,7 @@
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -41,6 +42,7 @@ struct opgpu_ctx {
     double *d_dg = nullptr, *d_pair_sigma = nullptr, *d_pair_mu = nullptr;
     double* d_dg_pair = nullptr;     // limited driving force per grain pair (G <= kMaxPairTableGrains)
     double* d_grot = nullptr;        // [G*9] grain rotation matrices (identity unless oriented)
+    double* d_facets = nullptr;      // FACETED: rows of (unit facet normal, SigmaF, EpsilonEF)
     // checkpoints of the state and the grain records (adjoint rollouts)
     struct Slot {
         uint8_t* cnt = nullptr; int16_t* idx = nullptr; void* val = nullptr;
@@ -329,6 +331,45 @@ double disorientation_cubic(const double* A, const double* B)
     return 2 * std::acos(m);
 }
 
+// The facet normals a FACETED facet (h, k, l) stands for: itself, or with $NfacetFamilies every
+// distinct vector of its family (index permutations with sign changes, the set that
+// Tools::findIndexPermutations enumerates, src/Tools.cpp:37-260), each normalised as
+// iVector3::normalized (include/Containers/iVector3.h:274-289).  The model takes the facet of
+// largest cos^2, so the order within a family does not matter.
+void facet_normals(long h, long k, long l, bool family, std::vector<double>& out)
+{
+    std::vector<std::array<long, 3>> v;
+    if (!family)
+        v.push_back({h, k, l});
+    else
+    {
+        const long a[3] = {std::labs(h), std::labs(k), std::labs(l)};
+        const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+        for (const auto& pm : perm)
+            for (int sg = 0; sg < 8; sg++)
+            {
+                std::array<long, 3> w = {a[pm[0]] * ((sg & 1) ? -1 : 1), a[pm[1]] * ((sg & 2) ? -1 : 1),
+                                         a[pm[2]] * ((sg & 4) ? -1 : 1)};
+                bool dup = false;
+                for (const auto& u : v) dup |= u == w;
+                if (!dup) v.push_back(w);
+            }
+    }
+    for (const auto& w : v)
+    {
+        const double norm = std::sqrt((double)(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]));
+        if (norm != 0.0)
+        {
+            const double inv = 1.0 / norm;
+            out.push_back(w[0] * inv); out.push_back(w[1] * inv); out.push_back(w[2] * inv);
+        }
+        else
+        {
+            out.push_back(0.0); out.push_back(0.0); out.push_back(0.0);
+        }
+    }
+}
+
 // InterfaceEnergyModel::CalculateDisorientation (include/InterfaceProperties/InterfaceEnergyModel.h:
 // 308-323): Read-Shockley-type energy of the disorientation angle, constant above 0.349066 rad.
 double disorientation_energy(const double* A, const double* B)
@@ -539,6 +580,7 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     dfree(ctx->d_slow_count);
     dfree(ctx->d_wl);
     dfree(ctx->d_bucket); dfree(ctx->d_bucket_count); dfree(ctx->d_bucket_off);
+    dfree(ctx->d_facets);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
     for (auto& s : ctx->slots)
@@ -568,6 +610,7 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
     sp.limiting = m->limiting;
     sp.tj_factor = m->tj_factor;
     sp.consider_nucleus_volume = m->consider_nucleus_volume;
+    std::vector<double> facet_rows;
     for (int a = 0; a < P; a++)
     for (int b = 0; b < P; b++)
     {
@@ -576,10 +619,10 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         sp.mu_p[q] = m->mu[q];
         const double lim = m->limit ? m->limit[q] : 0.95;   // src/DrivingForce.cpp:161
         const int model = m->energy_model ? m->energy_model[q] : 0;
-        if (model < 0 || model > 5)
-            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) .. 5 (HEXYANG)");
+        if (model < 0 || model > 6)
+            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) .. 6 (FACETED)");
         sp.emodel[q] = (signed char)model;
-        const bool normal_model = model == 1 || model >= 3;
+        const bool normal_model = model == 1 || (model >= 3 && model <= 5);
         sp.eps_p[q] = (normal_model && m->cubic_eps) ? m->cubic_eps[q] : 0.0;
         for (int k = 0; k < 3; k++) sp.eps_x[q][k] = (model >= 4 && m->model_eps) ? m->model_eps[3 * q + k] : 0.0;
         // DISORIENTATION reads no $Sigma: its Energy and MaxEnergy keep the constructor's 0
@@ -589,6 +632,31 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         // MaxEnergy: Energy for ISO and the HEX models (InterfaceEnergyModel.h:82, 105-134),
         // Energy*(1 + Epsilon*1.41) for CUBIC (ReadInputCubic, :87-94), 0 for DISORIENTATION
         sp.maxe_p[q] = model == 1 ? m->sigma[q] * (1.0 + sp.eps_p[q] * 1.41) : (model == 2 ? 0.0 : m->sigma[q]);
+        sp.facet_lo[q] = sp.facet_hi[q] = 0;
+        if (model == 6)
+        {
+            // ReadInputFaceted (InterfaceEnergyModel.h:196-246): facet rows, Energy = mean SigmaF
+            // (accumulated in facet order), MaxEnergy = max SigmaF
+            if (!m->facet_start || !m->facet_data || m->facet_start[q + 1] <= m->facet_start[q])
+                return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: a FACETED pair needs facets");
+            const int n0 = m->facet_start[q], n1 = m->facet_start[q + 1], nf = n1 - n0;
+            const bool family = m->facet_family && m->facet_family[q];
+            double energy = 0.0, maxe = 0.0;
+            sp.facet_lo[q] = (int)(facet_rows.size() / 5);
+            for (int f = n0; f < n1; f++)
+            {
+                const double* d = m->facet_data + 5 * (size_t)f;
+                std::vector<double> nrm;
+                facet_normals(std::lround(d[0]), std::lround(d[1]), std::lround(d[2]), family, nrm);
+                for (size_t r = 0; r < nrm.size(); r += 3)
+                    facet_rows.insert(facet_rows.end(), {nrm[r], nrm[r + 1], nrm[r + 2], d[3], d[4]});
+                energy += d[3] / nf;
+                if (d[3] > maxe) maxe = d[3];
+            }
+            sp.facet_hi[q] = (int)(facet_rows.size() / 5);
+            sp.sigma_p[q] = energy;
+            sp.maxe_p[q] = maxe;
+        }
         // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor
         double allowed = lim * sp.pref_df * sp.maxe_p[q];
         allowed *= m->regularization;
@@ -596,6 +664,13 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
     }
     sp.aniso = 0;   // models of the interface normal (the disorientation energy depends on the grain pair only)
     for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1 || sp.emodel[q] >= 3;
+    dfree(ctx->d_facets);
+    ctx->d_facets = nullptr;
+    if (!facet_rows.empty())
+    {
+        CK(dalloc(&ctx->d_facets, facet_rows.size()));
+        CK(cudaMemcpy(ctx->d_facets, facet_rows.data(), facet_rows.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     for (int a = 0; a < P; a++) sp.solid_p[a] = (signed char)(m->phase_solid ? (m->phase_solid[a] != 0) : 1);
     ctx->nvf = m->nucleus_volume_factor > 0.0 ? m->nucleus_volume_factor : 1.0;
     ctx->model_set = true;
@@ -941,7 +1016,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
         a.vr = ctx->d_vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
         a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
         a.dg_pair = pair_table ? ctx->d_dg_pair : nullptr;
-        a.grot = ctx->d_grot;
+        a.grot = ctx->d_grot; a.facets = ctx->d_facets;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
         a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
@@ -1235,7 +1310,7 @@ StepArrays step_arrays(opgpu_ctx* ctx, const uint8_t* cnt_in, const int16_t* idx
     a.vr = vr; a.gphase = ctx->d_gphase; a.gstage = ctx->d_gstage;
     a.dg = ctx->d_dg; a.pair_sigma = ctx->d_pair_sigma; a.pair_mu = ctx->d_pair_mu;
     a.dg_pair = (ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && !ctx->dg_pair_dirty) ? ctx->d_dg_pair : nullptr;
-    a.grot = ctx->d_grot;
+    a.grot = ctx->d_grot; a.facets = ctx->d_facets;
     a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
     return a;
 }

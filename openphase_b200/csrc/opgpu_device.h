@@ -75,6 +75,7 @@ struct StepParams {
     signed char emodel[kMaxPhases * kMaxPhases];
     double eps_p[kMaxPhases * kMaxPhases];
     double eps_x[kMaxPhases * kMaxPhases][3];
+    int facet_lo[kMaxPhases * kMaxPhases], facet_hi[kMaxPhases * kMaxPhases];   // FACETED: rows of facets
     double maxe_p[kMaxPhases * kMaxPhases];
     signed char solid_p[kMaxPhases];
     int ngs;
@@ -124,6 +125,7 @@ struct StepArrays {
     unsigned* bucket_count;    // [kListCap + 1][max blocks] entries per slice
     unsigned* bucket_off;      // [kListCap + 1][blocks + 1] exclusive prefix of bucket_count per list
                                // length, then the length's total
+    const double* facets;      // FACETED: rows of (unit facet normal x, y, z, SigmaF, EpsilonEF)
     long long bucket_cap;
     int slice;                 // entries per classify-block slice
 };

@@ -141,8 +141,9 @@ __device__ __forceinline__ void interface_orientation(const double* g3, const do
 
 // InterfaceEnergyModel::Calculate (include/InterfaceProperties/InterfaceEnergyModel.h:325-399) for
 // the models of the interface normal n: CUBIC, HEXBOETTGER (Boettger et al. 2006), HEXSUN (Sun et
-// al. 2006) and HEXYANG (Yang et al. 2015), in the reference's operation order.
-__device__ __forceinline__ double model_energy(const StepParams& p, int q, const double* n)
+// al. 2006), HEXYANG (Yang et al. 2015) and FACETED (facet rows: unit normal, SigmaF, EpsilonEF),
+// in the reference's operation order.
+__device__ __forceinline__ double model_energy(const StepParams& p, int q, const double* n, const double* facets)
 {
     const double E = p.sigma_p[q], e1 = p.eps_p[q];
     const double x = n[0], y = n[1], z = n[2];
@@ -166,6 +167,21 @@ __device__ __forceinline__ double model_energy(const StepParams& p, int q, const
             const double e2 = p.eps_x[q][0], e3 = p.eps_x[q][1];
             return E * (1.0 + e1 * pow((3.0 * z * z - 1.0), 2.0)
                         + e2 * pow((x * x * x - 3.0 * x * y * y), 2.0) * pow((9.0 * z * z - 1.0 + e3), 2.0));
+        }
+        case 6:
+        {
+            // FACETED (Salama et al. 2020): the facet of largest cos^2 of its inclination sets the
+            // energy EnergyA*EpsilonA^2*(sin^2 + EpsilonA^2 cos^2)^(-3/2)
+            double cos2 = 0.0, ea = 0.0, epa = 0.0;
+            for (int f = p.facet_lo[q]; f < p.facet_hi[q]; f++)
+            {
+                const double* r = facets + 5 * f;
+                const double c = x * r[0] + y * r[1] + z * r[2];
+                const double c2 = c * c;
+                if (c2 > cos2) { cos2 = c2; ea = r[3]; epa = r[4]; }
+            }
+            const double sin2 = 1.0 - cos2;
+            return ea * epa * epa * pow(sqrt(sin2 + epa * epa * cos2), -3.0);
         }
         default:
             return E * (1.0 + e1 * (1.5 - 2.5 * (pow(x, 4.0) + pow(y, 4.0) + pow(z, 4.0))));
@@ -194,7 +210,7 @@ __device__ __forceinline__ double voxel_energy(const StepParams& p, const StepAr
             const double g3[3] = {(double)sc.grad[(3 * i) * S], (double)sc.grad[(3 * i + 1) * S], (double)sc.grad[(3 * i + 2) * S]};
             double n[3];
             interface_orientation(g3, a.grot + 9 * (long long)gi, n);
-            loc += model_energy(p, q, n) * wA;
+            loc += model_energy(p, q, n, a.facets) * wA;
         }
         else wA = 0.0;
     }
@@ -207,7 +223,7 @@ __device__ __forceinline__ double voxel_energy(const StepParams& p, const StepAr
             const double g3[3] = {(double)sc.grad[(3 * j) * S], (double)sc.grad[(3 * j + 1) * S], (double)sc.grad[(3 * j + 2) * S]};
             double n[3];
             interface_orientation(g3, a.grot + 9 * (long long)gj, n);
-            loc += model_energy(p, q, n) * wB;
+            loc += model_energy(p, q, n, a.facets) * wB;
         }
         else wB = 0.0;
     }

@@ -29,7 +29,8 @@ class OpParams(C.Structure):
                 ("stencil", C.c_int), ("gradient_stencil", C.c_int), ("nphases", C.c_int), ("ngrains", C.c_int),
                 ("grain_phase", C.c_void_p), ("phase_solid", C.c_void_p), ("sigma_phase", C.c_void_p),
                 ("mu_phase", C.c_void_p), ("energy_model", C.c_void_p), ("cubic_eps", C.c_void_p),
-                ("model_eps", C.c_void_p), ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
+                ("model_eps", C.c_void_p), ("facet_start", C.c_void_p), ("facet_data", C.c_void_p),
+                ("facet_family", C.c_void_p), ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
                 ("limiting", C.c_int), ("limit_phase", C.c_void_p), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int),
                 ("nucleus_volume_factor", C.c_double), ("threads", C.c_int)]
@@ -103,6 +104,8 @@ class Oracle:
         eps = keep(eps) if eps is not None else None
         meps = case.model_eps()
         meps = keep(meps) if meps is not None else None
+        fac = case.facet_tables()
+        fac = tuple(keep(x) for x in fac) if fac is not None else None
         quat = case.quaternions()
         quat = keep(quat.astype(np.float64)) if quat is not None else None
         ps = case.pair_sigma()
@@ -116,6 +119,8 @@ class Oracle:
                      energy_model=_p(em).value if em is not None else None,
                      cubic_eps=_p(eps).value if eps is not None else None,
                      model_eps=_p(meps).value if meps is not None else None,
+                     facet_start=_p(fac[0]).value if fac else None, facet_data=_p(fac[1]).value if fac else None,
+                     facet_family=_p(fac[2]).value if fac else None,
                      quat=_p(quat).value if quat is not None else None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
                      dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
                      limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
@@ -198,6 +203,11 @@ def _case_text(case, workdir: Path, dump_steps, threads):
                       f"limit {a} {b} {float(lim[a, b])!r}"]
             if case.disorientation:
                 lines.append(f"energy_model {a} {b} DISORIENTATION")
+            elif case.facets and eps is not None and eps[a, b] != 0.0:
+                lines.append(f"energy_model {a} {b} FACETED")
+                lines.append(f"facet_family {a} {b} {int(case.facet_families)}")
+                for (h, k, l, sf, ef) in case.facets:
+                    lines.append(f"facet {a} {b} {h} {k} {l} {float(sf)!r} {float(ef)!r}")
             elif eps is not None and eps[a, b] != 0.0:
                 name = case.hex_model or "CUBIC"
                 lines += [f"energy_model {a} {b} {name}", f"cubic_eps {a} {b} {float(eps[a, b])!r}"]

@@ -35,6 +35,9 @@ struct op_sim {
     int* energy_model;            /* [P*P] OP_ENERGY_*                                           */
     double* cubic_eps;            /* [P*P] Epsilon1                                              */
     double* model_eps;            /* [P*P*3] Epsilon2..4                                         */
+    double* facets;               /* FACETED rows: unit facet normal (3), SigmaF, EpsilonEF      */
+    int* facet_lo; int* facet_hi; /* [P*P] rows of each pair                                     */
+    double* phase_e; double* phase_maxe;   /* [P*P] FACETED Energy (mean SigmaF), MaxEnergy      */
     double* rot;                  /* [G*9] grain RotationMatrix, row-major                       */
     double* quat;                 /* [G*4] grain Orientation (s, x, y, z) as given               */
     int aniso;                    /* some phase pair uses an anisotropic energy model            */
@@ -51,6 +54,28 @@ struct op_sim {
 };
 
 static double dmax(double a, double b) { return (a < b) ? b : a; }   /* std::max */
+
+/* The facet vectors a FACETED facet (h, k, l) stands for: itself, or with facet families every
+ * distinct vector of its family (index permutations with sign changes, the set
+ * Tools::findIndexPermutations enumerates, src/Tools.cpp:37-260).  Returns their number (<= 48). */
+static int facet_family_vectors(long h, long k, long l, int family, long w[48][3])
+{
+    if (!family) { w[0][0] = h; w[0][1] = k; w[0][2] = l; return 1; }
+    const long a[3] = {labs(h), labs(k), labs(l)};
+    static const int perm[6][3] = {{0,1,2},{0,2,1},{1,0,2},{1,2,0},{2,0,1},{2,1,0}};
+    int n = 0;
+    for (int pm = 0; pm < 6; pm++)
+    for (int sg = 0; sg < 8; sg++)
+    {
+        const long v0 = a[perm[pm][0]]*((sg & 1) ? -1 : 1);
+        const long v1 = a[perm[pm][1]]*((sg & 2) ? -1 : 1);
+        const long v2 = a[perm[pm][2]]*((sg & 4) ? -1 : 1);
+        int dup = 0;
+        for (int i = 0; i < n; i++) dup |= (w[i][0] == v0 && w[i][1] == v1 && w[i][2] == v2);
+        if (!dup) { w[n][0] = v0; w[n][1] = v1; w[n][2] = v2; n++; }
+    }
+    return n;
+}
 static double dmin(double a, double b) { return (b < a) ? b : a; }   /* std::min */
 
 static double* dup_d(const double* src, size_t n)
@@ -147,6 +172,53 @@ op_sim* op_create(const op_params* p, int cap)
     s->cubic_eps = (double*)calloc((size_t)P*P, sizeof(double));
     s->model_eps = (double*)calloc((size_t)P*P*3, sizeof(double));
     if (p->model_eps) memcpy(s->model_eps, p->model_eps, (size_t)P*P*3*sizeof(double));
+    /* ReadInputFaceted (InterfaceEnergyModel.h:196-246): facet normals (families expanded), Energy
+     * = mean SigmaF accumulated in facet order, MaxEnergy = max SigmaF */
+    s->facet_lo = (int*)calloc((size_t)P*P, sizeof(int));
+    s->facet_hi = (int*)calloc((size_t)P*P, sizeof(int));
+    s->phase_e = (double*)calloc((size_t)P*P, sizeof(double));
+    s->phase_maxe = (double*)calloc((size_t)P*P, sizeof(double));
+    s->facets = NULL;
+    {
+        int rows = 0, cap_rows = 0;
+        for (int q = 0; q < P*P; q++)
+        {
+            if (!p->energy_model || p->energy_model[q] != OP_ENERGY_FACETED || !p->facet_start) continue;
+            const int n0 = p->facet_start[q], n1 = p->facet_start[q + 1], nf = n1 - n0;
+            const int family = p->facet_family ? p->facet_family[q] : 0;
+            double energy = 0.0, maxe = 0.0;
+            s->facet_lo[q] = rows;
+            for (int f = n0; f < n1; f++)
+            {
+                const double* d = p->facet_data + 5*(size_t)f;
+                long w[48][3];
+                const int nw = facet_family_vectors(lround(d[0]), lround(d[1]), lround(d[2]), family, w);
+                if (rows + nw > cap_rows)
+                {
+                    cap_rows = 2*(rows + nw);
+                    s->facets = (double*)realloc(s->facets, (size_t)cap_rows*5*sizeof(double));
+                }
+                for (int k = 0; k < nw; k++)
+                {
+                    double* r = s->facets + 5*(size_t)rows++;
+                    /* iVector3::normalized (include/Containers/iVector3.h:274-289) */
+                    const double norm = sqrt((double)(w[k][0]*w[k][0] + w[k][1]*w[k][1] + w[k][2]*w[k][2]));
+                    if (norm != 0.0)
+                    {
+                        const double inv = 1.0/norm;
+                        r[0] = w[k][0]*inv; r[1] = w[k][1]*inv; r[2] = w[k][2]*inv;
+                    }
+                    else { r[0] = 0.0; r[1] = 0.0; r[2] = 0.0; }
+                    r[3] = d[3]; r[4] = d[4];
+                }
+                energy += d[3]/nf;
+                if (d[3] > maxe) maxe = d[3];
+            }
+            s->facet_hi[q] = rows;
+            s->phase_e[q] = energy;
+            s->phase_maxe[q] = maxe;
+        }
+    }
     s->aniso = 0;
     for (int q = 0; q < P*P; q++)
     {
@@ -228,6 +300,7 @@ void op_destroy(op_sim* s)
     free(s->sigma_phase); free(s->mu_phase); free(s->limit_phase);
     free(s->pair_sigma); free(s->pair_mu); free(s->dg);
     free(s->energy_model); free(s->cubic_eps); free(s->model_eps); free(s->rot); free(s->quat);
+    free(s->facets); free(s->facet_lo); free(s->facet_hi); free(s->phase_e); free(s->phase_maxe);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
     free(s->exist); free(s->stage);
@@ -288,6 +361,7 @@ static double phase_energy(const op_sim* s, int pa, int pb)
 {
     const int q = pa*s->p.nphases + pb;
     if (s->energy_model[q] == OP_ENERGY_DISORIENTATION) return 0.0;
+    if (s->energy_model[q] == OP_ENERGY_FACETED) return s->phase_e[q];
     return s->sigma_phase[q];
 }
 
@@ -298,6 +372,7 @@ static double phase_max_energy(const op_sim* s, int pa, int pb)
     const int q = pa*s->p.nphases + pb;
     if (s->energy_model[q] == OP_ENERGY_CUBIC) return s->sigma_phase[q]*(1.0 + s->cubic_eps[q]*1.41);
     if (s->energy_model[q] == OP_ENERGY_DISORIENTATION) return 0.0;   /* MaxEnergy keeps its 0 */
+    if (s->energy_model[q] == OP_ENERGY_FACETED) return s->phase_maxe[q];
     return s->sigma_phase[q];
 }
 
@@ -390,6 +465,20 @@ static double model_energy(const op_sim* s, int q, const double n[3])
                       + ex[0]*3.0/16.0/sqrt(OP_PI)*(35.0*pow(z, 4) - 30.0*z*z + 3.0)
                       + ex[1]*sqrt(13.0/OP_PI)/32.0*(231.0*pow(z, 6) - 315.0*pow(z, 4) + 105.0*z*z - 5.0)
                       + ex[2]*sqrt(6006.0/OP_PI)/64.0*(pow(x, 6) - 15.0*pow(x, 4)*y*y + 15.0*x*x*pow(y, 4) - pow(y, 6)));
+        case OP_ENERGY_FACETED:
+        {
+            /* InterfaceEnergyModel::Calculate, Faceted (:417-438): the facet of largest cos^2 */
+            double cos2 = 0.0, ea = 0.0, epa = 0.0;
+            for (int f = s->facet_lo[q]; f < s->facet_hi[q]; f++)
+            {
+                const double* r = s->facets + 5*f;
+                const double c = x*r[0] + y*r[1] + z*r[2];
+                const double c2 = c*c;
+                if (c2 > cos2) { cos2 = c2; ea = r[3]; epa = r[4]; }
+            }
+            const double sin2 = 1.0 - cos2;
+            return ea*epa*epa*pow(sqrt(sin2 + epa*epa*cos2), -3.0);
+        }
         case OP_ENERGY_HEXYANG:
             return E*(1.0 + e1*pow((3.0*z*z - 1.0), 2) + ex[0]*pow((x*x*x - 3.0*x*y*y), 2)*pow((9.0*z*z - 1.0 + ex[1]), 2));
         default:   /* CUBIC */

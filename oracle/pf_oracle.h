@@ -20,7 +20,7 @@ extern "C" {
 enum { OP_STENCIL_SIMPLE = 0, OP_STENCIL_ISOTROPIC = 1, OP_STENCIL_LB = 2 };
 enum { OP_STAGE_STABLE = 0, OP_STAGE_SEED = 1, OP_STAGE_NUCLEUS = 2 };
 enum { OP_ENERGY_ISO = 0, OP_ENERGY_CUBIC = 1, OP_ENERGY_DISORIENTATION = 2, OP_ENERGY_HEXBOETTGER = 3,
-       OP_ENERGY_HEXSUN = 4, OP_ENERGY_HEXYANG = 5 };
+       OP_ENERGY_HEXSUN = 4, OP_ENERGY_HEXYANG = 5, OP_ENERGY_FACETED = 6 };
 
 /* Status bits reported by op_step (OR-ed over all voxels and steps since the last call). */
 enum {
@@ -45,6 +45,9 @@ typedef struct op_params {
     const int* energy_model;          /* [P*P] OP_ENERGY_* (NULL: all ISO)                      */
     const double* cubic_eps;          /* [P*P] Epsilon1 of the CUBIC / HEX models (NULL: 0)     */
     const double* model_eps;          /* [P*P*3] Epsilon2..4 of the HEX models (NULL: 0)        */
+    const int* facet_start;           /* [P*P+1] FACETED: facets of pair q in facet_data rows    */
+    const double* facet_data;         /* rows of h, k, l, SigmaF, EpsilonEF                       */
+    const int* facet_family;          /* [P*P] 1: facets stand for their families                */
     const double* quat;               /* [G*4] grain orientation quaternions (w,x,y,z) or NULL  */
     const double* pair_sigma;         /* [G*G] per-grain-pair sigma overriding the phase value, or NULL */
     const double* pair_mu;            /* [G*G] per-grain-pair mobility, or NULL                 */

@@ -58,6 +58,8 @@ struct Case
     std::vector<double> quat;      // [G*4] grain orientations (s, x, y, z), empty: none
     std::map<std::pair<int,int>, double> sigma, mu, limit, cubic_eps;
     std::map<std::pair<int,int>, std::vector<double>> model_eps;   // Epsilon2..4 of the HEX models
+    std::map<std::pair<int,int>, std::vector<std::vector<double>>> facets;   // FACETED: h k l SigmaF EpsilonEF
+    std::map<std::pair<int,int>, int> facet_family;
     std::map<std::pair<int,int>, std::string> energy_model;
     int ngrains = 0;
     std::vector<int> grain_phase;
@@ -119,6 +121,8 @@ static Case parse_case(const std::string& path)
         else if (key == "limit") { int a, b; double v; is >> a >> b >> v; c.limit[{a,b}] = v; }
         else if (key == "energy_model") { int a, b; std::string m; is >> a >> b >> m; c.energy_model[{a,b}] = m; }
         else if (key == "cubic_eps") { int a, b; double v; is >> a >> b >> v; c.cubic_eps[{a,b}] = v; }
+        else if (key == "facet_family") { int a, b, f; is >> a >> b >> f; c.facet_family[{a,b}] = f; }
+        else if (key == "facet") { int a, b; std::vector<double> f(5); is >> a >> b >> f[0] >> f[1] >> f[2] >> f[3] >> f[4]; c.facets[{a,b}].push_back(f); }
         else if (key == "model_eps") { int a, b; double e2, e3, e4; is >> a >> b >> e2 >> e3 >> e4; c.model_eps[{a,b}] = {e2, e3, e4}; }
         else if (key == "ngrains") is >> c.ngrains;
         else if (key == "grain_phase_file") is >> grain_phase_file;
@@ -180,6 +184,16 @@ static void write_opi(const Case& c, const std::string& path)
         if (model == "HEXSUN")
             o << "$EpsilonE20_" << ab << " : " << e1 << "\n" << "$EpsilonE40_" << ab << " : " << ex[0] << "\n"
               << "$EpsilonE60_" << ab << " : " << ex[1] << "\n" << "$EpsilonE66_" << ab << " : " << ex[2] << "\n";
+        if (model == "FACETED")
+        {
+            const auto& fs = c.facets.at({a,b});
+            const bool fam = c.facet_family.count({a,b}) and c.facet_family.at({a,b});
+            o << (fam ? "$NfacetFamilies_" : "$Nfacets_") << ab << " : " << fs.size() << "\n";
+            for (size_t n = 0; n < fs.size(); n++)
+                o << "$Facet_" << ab << "_" << n << " : " << (long)fs[n][0] << " " << (long)fs[n][1] << " " << (long)fs[n][2] << "\n"
+                  << "$SigmaF_" << ab << "_" << n << " : " << fs[n][3] << "\n"
+                  << "$EpsilonEF_" << ab << "_" << n << " : " << fs[n][4] << "\n";
+        }
         if (model == "HEXYANG")
             o << "$EpsilonE1_" << ab << " : " << e1 << "\n" << "$EpsilonE2_" << ab << " : " << ex[0] << "\n"
               << "$EpsilonE3_" << ab << " : " << ex[1] << "\n";

@@ -53,6 +53,13 @@ GOLDEN_CASES = {
                                phase_solid=(0, 1), phase_cubic_eps=((0.0, -0.03), (-0.03, 0.0)),
                                phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
                                hex_model="HEXYANG", hex_eps=(0.1, 0.2, 0.0), name="hexyang_nuclei_24"), [1, 30]),
+    # FACETED energy model ({100} and {111} facet families) on the solid-liquid pairs
+    "faceted_nuclei_24": (Case(24, 24, 24, 7, seed=7, iwidth=5.0, dt=0.05, sigma=1.2,
+                               phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                               phase_solid=(0, 1), phase_cubic_eps=((0.0, 1.0), (1.0, 0.0)),
+                               phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                               facets=((1, 0, 0, 1.0, 0.7), (1, 1, 1, 1.1, 0.8)), name="faceted_nuclei_24"),
+                          [1, 10, 30]),
     # DISORIENTATION energy model: per-grain-pair energies from the cubic disorientation of
     # orientations spread over up to 0.6 rad (pairs below and above the 0.349 rad cap)
     "disorientation_20": (Case(20, 20, 20, 12, seed=11, iwidth=4.0, dt=0.1, orientations=True,
