@@ -101,6 +101,13 @@ typedef struct opgpu_model {
     const int32_t* facet_start;    /* [P*P+1]                                                      */
     const double* facet_data;      /* [facet_start[P*P]*5]                                         */
     const int32_t* facet_family;   /* [P*P]                                                        */
+    /* Anisotropic interface mobility (InterfaceMobilityModel.h:71-113, 210-265; InterfaceProperties.cpp:
+     * 680-707): per phase pair 0 = ISO, 1 = CUBIC, 3 = HEXBOETTGER, 4 = HEXSUN, 5 = HEXYANG
+     * ($MobilityModel_a_b) and Epsilon1..4 ($EpsilonM_a_b; HEXSUN $EpsilonM20/40/60/66_a_b; HEXYANG
+     * $EpsilonM1/2/3_a_b).  Per voxel and pair the model is summed over the solid grains whose value
+     * is neither 0 nor 1 (not averaged, as in the reference), else Mobility.  NULL: all ISO.      */
+    const int32_t* mobility_model; /* [P*P]                                                        */
+    const double* mobility_eps;    /* [P*P*4]                                                      */
 } opgpu_model;
 
 typedef struct opgpu_stats {

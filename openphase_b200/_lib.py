@@ -62,7 +62,8 @@ class Model(C.Structure):
                 ("nucleus_volume_factor", C.c_double), ("energy_model", C.POINTER(C.c_int32)),
                 ("cubic_eps", C.POINTER(C.c_double)), ("phase_solid", C.POINTER(C.c_int32)),
                 ("model_eps", C.POINTER(C.c_double)), ("facet_start", C.POINTER(C.c_int32)),
-                ("facet_data", C.POINTER(C.c_double)), ("facet_family", C.POINTER(C.c_int32))]
+                ("facet_data", C.POINTER(C.c_double)), ("facet_family", C.POINTER(C.c_int32)),
+                ("mobility_model", C.POINTER(C.c_int32)), ("mobility_eps", C.POINTER(C.c_double))]
 
 
 class Stats(C.Structure):

@@ -59,6 +59,8 @@ class Case:
     hex_eps: tuple = (0.0, 0.0, 0.0)           # Epsilon2..4 of the HEX model (Epsilon1: phase_cubic_eps)
     facets: tuple = ()                         # FACETED in place of CUBIC: (h, k, l, SigmaF, EpsilonEF) each
     facet_families: bool = True                # every facet stands for its family of permutations
+    mobility_model: str = ""                   # CUBIC / HEXBOETTGER / HEXSUN / HEXYANG mobility on the pairs
+    mobility_eps: tuple = (0.0, 0.0, 0.0, 0.0)  # with anisotropic energy (phase_cubic_eps != 0): Epsilon1..4
 
     @property
     def n(self) -> int:
@@ -92,6 +94,18 @@ class Case:
             return None
         code = 6 if self.facets else {"": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.hex_model]
         return np.where(e != 0.0, code, 0).astype(np.int32)
+
+    def mobility_models(self) -> Optional[np.ndarray]:
+        """P x P mobility model codes (0 ISO, 1 CUBIC, 3..5 HEX*)."""
+        if not self.mobility_model or self.phase_cubic_eps is None:
+            return None
+        code = {"CUBIC": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.mobility_model]
+        return np.where(np.array(self.phase_cubic_eps) != 0.0, code, 0).astype(np.int32)
+
+    def mobility_eps_table(self) -> Optional[np.ndarray]:
+        if self.mobility_models() is None:
+            return None
+        return np.broadcast_to(np.asarray(self.mobility_eps, dtype=np.float64), (self.nphases, self.nphases, 4)).copy()
 
     def facet_tables(self):
         """(facet_start[P*P+1], facet_data[F, 5], facet_family[P*P]) for the FACETED pairs, or None."""

@@ -58,7 +58,7 @@ class Context:
     # ---- parameters
     def set_model(self, sigma, mu, *, limit=None, limiting=True, regularization=1.0, tj_factor=0.0,
                   consider_nucleus_volume=True, nucleus_volume_factor=1.0, energy_model=None, cubic_eps=None,
-                  phase_solid=None, model_eps=None, facets=None):
+                  phase_solid=None, model_eps=None, facets=None, mobility_model=None, mobility_eps=None):
         """facets: (facet_start[P*P+1], facet_data[F, 5], facet_family[P*P]) of the FACETED pairs."""
         sigma = np.ascontiguousarray(np.atleast_2d(sigma), dtype=np.float64)
         mu = np.ascontiguousarray(np.atleast_2d(mu), dtype=np.float64)
@@ -67,6 +67,8 @@ class Context:
         eps = None if cubic_eps is None else np.ascontiguousarray(cubic_eps, dtype=np.float64)
         sol = None if phase_solid is None else np.ascontiguousarray(phase_solid, dtype=np.int32)
         meps = None if model_eps is None else np.ascontiguousarray(model_eps, dtype=np.float64)
+        mm = None if mobility_model is None else np.ascontiguousarray(mobility_model, dtype=np.int32)
+        mme = None if mobility_eps is None else np.ascontiguousarray(mobility_eps, dtype=np.float64)
         fs, fd, ff = (None, None, None) if facets is None else (
             np.ascontiguousarray(facets[0], dtype=np.int32), np.ascontiguousarray(facets[1], dtype=np.float64),
             np.ascontiguousarray(facets[2], dtype=np.int32))
@@ -77,7 +79,8 @@ class Context:
                   nucleus_volume_factor=nucleus_volume_factor, energy_model=as_ptr(em, C.c_int32),
                   cubic_eps=as_ptr(eps, C.c_double), phase_solid=as_ptr(sol, C.c_int32),
                   model_eps=as_ptr(meps, C.c_double), facet_start=as_ptr(fs, C.c_int32),
-                  facet_data=as_ptr(fd, C.c_double), facet_family=as_ptr(ff, C.c_int32))
+                  facet_data=as_ptr(fd, C.c_double), facet_family=as_ptr(ff, C.c_int32),
+                  mobility_model=as_ptr(mm, C.c_int32), mobility_eps=as_ptr(mme, C.c_double))
         _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
 
     def set_orientations(self, quat):
@@ -261,7 +264,8 @@ class Context:
         ctx.set_model(case.sigma_phase(), case.mu_phase(), limit=case.limit_phase(), limiting=case.limiting,
                       regularization=case.regularization, tj_factor=case.tj_factor,
                       energy_model=case.energy_models(), cubic_eps=case.cubic_eps(), phase_solid=case.solid_phase(),
-                      model_eps=case.model_eps(), facets=case.facet_tables())
+                      model_eps=case.model_eps(), facets=case.facet_tables(),
+                      mobility_model=case.mobility_models(), mobility_eps=case.mobility_eps_table())
         ctx.set_grains(case.ngrains, phase=case.grain_phase())
         if case.orientations:
             ctx.set_orientations(case.quaternions())

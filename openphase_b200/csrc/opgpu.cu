@@ -662,8 +662,16 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         allowed *= m->regularization;
         sp.allowed_p[q] = allowed;
     }
+    for (int q = 0; q < P * P; q++)
+    {
+        const int mm = m->mobility_model ? m->mobility_model[q] : 0;
+        if (mm != 0 && mm != 1 && (mm < 3 || mm > 5))
+            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: mobility model 0 (ISO), 1 (CUBIC), 3..5 (HEX*)");
+        sp.mmodel[q] = (signed char)mm;
+        for (int k = 0; k < 4; k++) sp.meps[q][k] = (mm != 0 && m->mobility_eps) ? m->mobility_eps[4 * q + k] : 0.0;
+    }
     sp.aniso = 0;   // models of the interface normal (the disorientation energy depends on the grain pair only)
-    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1 || sp.emodel[q] >= 3;
+    for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1 || sp.emodel[q] >= 3 || sp.mmodel[q] != 0;
     dfree(ctx->d_facets);
     ctx->d_facets = nullptr;
     if (!facet_rows.empty())

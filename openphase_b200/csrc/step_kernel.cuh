@@ -188,6 +188,66 @@ __device__ __forceinline__ double model_energy(const StepParams& p, int q, const
     }
 }
 
+// InterfaceMobilityModel::Calculate (include/InterfaceProperties/InterfaceMobilityModel.h:210-265):
+// CUBIC, HEXBOETTGER, HEXSUN, HEXYANG of the interface normal n, in the reference's operation order
+// (the signs of the anisotropy terms differ from the energy models').
+__device__ __forceinline__ double mobility_model(const StepParams& p, int q, const double* n)
+{
+    const double M = p.mu_p[q], e1 = p.meps[q][0], e2 = p.meps[q][1], e3 = p.meps[q][2], e4 = p.meps[q][3];
+    const double x = n[0], y = n[1], z = n[2];
+    switch (p.mmodel[q])
+    {
+        case 3:
+            return M * (1.0 + e1 * (pow(x, 6.0) - pow(y, 6.0) - 15.0 * pow(x, 4.0) * y * y + 15.0 * pow(y, 4.0) * x * x
+                                    + (5.0 * pow(z, 4.0) - 5.0 * pow(z, 2.0) + pow(z, 6.0))));
+        case 4:
+        {
+            const double pi = 3.14159265358979323846;
+            return M * (1.0 - e1 * sqrt(5.0 / 16.0 / pi) * (3.0 * z * z - 1.0)
+                        - e2 * 3.0 / 16.0 / sqrt(pi) * (35.0 * pow(z, 4.0) - 30.0 * z * z + 3.0)
+                        - e3 * sqrt(13.0 / pi) / 32.0 * (231.0 * pow(z, 6.0) - 315.0 * pow(z, 4.0) + 105.0 * z * z - 5.0)
+                        - e4 * sqrt(6006.0 / pi) / 64.0
+                              * (pow(x, 6.0) - 15.0 * pow(x, 4.0) * y * y + 15.0 * x * x * pow(y, 4.0) - pow(y, 6.0)));
+        }
+        case 5:
+            return M * (1.0 - e1 * pow((3.0 * z * z - 1.0), 2.0)
+                        - e2 * pow((x * x * x - 3.0 * x * y * y), 2.0) * pow((9.0 * z * z - 1.0 + e3), 2.0));
+        default:
+            return M * (1.0 - e1 * (1.5 - 2.5 * (pow(x, 4.0) + pow(y, 4.0) + pow(z, 4.0))));
+    }
+}
+
+// The interface mobility of the pair (i, j) of a voxel's list as InterfaceProperties::SetSR stores
+// it (src/InterfaceProperties.cpp:680-707): ISO (or the per-grain-pair table), or the anisotropic
+// model summed over the solid grains whose value is neither 0 nor 1 (Mobility when there is none).
+template <class R>
+__device__ __forceinline__ double voxel_mobility(const StepParams& p, const StepArrays& a, const ListScratch<R>& sc,
+                                                 int i, int j)
+{
+    const int S = sc.stride;
+    const int gi = sc.g[i * S], gj = sc.g[j * S];
+    const int pA = a.gphase[gi], pB = a.gphase[gj];
+    const int q = pA * p.nphases + pB;
+    if (p.mmodel[q] == 0) return pair_mobility(p, a, gi, gj);
+    double loc = 0.0;
+    int solids = 0;
+    for (int side = 0; side < 2; side++)
+    {
+        const int e = side == 0 ? i : j;
+        const int g = side == 0 ? gi : gj;
+        if (!p.solid_p[side == 0 ? pA : pB]) continue;
+        const double v = (double)sc.val[e * S];
+        if (v == 0.0 || v == 1.0) continue;
+        const double g3[3] = {(double)sc.grad[(3 * e) * S], (double)sc.grad[(3 * e + 1) * S], (double)sc.grad[(3 * e + 2) * S]};
+        double n[3];
+        interface_orientation(g3, a.grot + 9 * (long long)g, n);
+        loc += mobility_model(p, q, n);
+        solids++;
+    }
+    if (solids == 0) loc = p.mu_p[q];
+    return loc;
+}
+
 // The interface energy of the pair (i, j) of a voxel's list as InterfaceProperties::SetSR stores it
 // (src/InterfaceProperties.cpp:617-673): the ISO value, or the anisotropic model averaged over the
 // solid grains' interface orientations with weights |phi(1 - phi)| (MaxEnergy when no weight counts).
@@ -297,7 +357,7 @@ __device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& 
                     }
                 }
             }
-            dphi *= (R)pair_mobility(p, a, gi, gj) * norm_1 * scale;
+            dphi *= (R)(p.aniso ? voxel_mobility<R>(p, a, sc, i, j) : pair_mobility(p, a, gi, gj)) * norm_1 * scale;
             PV_(q) = (double)dphi;
         }
     }
@@ -314,7 +374,8 @@ __device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& 
                 const double locdG = limited_force(p, a, gi, gj);
                 double norm = sqrt(vi * (double)V_(j));
                 if (a.gstage[gi] == 1 || a.gstage[gj] == 1) norm += 1.0e-6;
-                const double dpsi = locdG * (double)(R)pair_mobility(p, a, gi, gj) * norm * p.pref_df;
+                const double mob = p.aniso ? voxel_mobility<R>(p, a, sc, i, j) : pair_mobility(p, a, gi, gj);
+                const double dpsi = locdG * (double)(R)mob * norm * p.pref_df;
                 PV_(pair_pos(i, j, n)) += dpsi;
             }
         }

@@ -30,7 +30,8 @@ class OpParams(C.Structure):
                 ("grain_phase", C.c_void_p), ("phase_solid", C.c_void_p), ("sigma_phase", C.c_void_p),
                 ("mu_phase", C.c_void_p), ("energy_model", C.c_void_p), ("cubic_eps", C.c_void_p),
                 ("model_eps", C.c_void_p), ("facet_start", C.c_void_p), ("facet_data", C.c_void_p),
-                ("facet_family", C.c_void_p), ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
+                ("facet_family", C.c_void_p), ("mobility_model", C.c_void_p), ("mobility_eps", C.c_void_p),
+                ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
                 ("limiting", C.c_int), ("limit_phase", C.c_void_p), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int),
                 ("nucleus_volume_factor", C.c_double), ("threads", C.c_int)]
@@ -106,6 +107,10 @@ class Oracle:
         meps = keep(meps) if meps is not None else None
         fac = case.facet_tables()
         fac = tuple(keep(x) for x in fac) if fac is not None else None
+        mm = case.mobility_models()
+        mm = keep(mm) if mm is not None else None
+        mme = case.mobility_eps_table()
+        mme = keep(mme) if mme is not None else None
         quat = case.quaternions()
         quat = keep(quat.astype(np.float64)) if quat is not None else None
         ps = case.pair_sigma()
@@ -121,6 +126,8 @@ class Oracle:
                      model_eps=_p(meps).value if meps is not None else None,
                      facet_start=_p(fac[0]).value if fac else None, facet_data=_p(fac[1]).value if fac else None,
                      facet_family=_p(fac[2]).value if fac else None,
+                     mobility_model=_p(mm).value if mm is not None else None,
+                     mobility_eps=_p(mme).value if mme is not None else None,
                      quat=_p(quat).value if quat is not None else None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
                      dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
                      limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
@@ -213,6 +220,13 @@ def _case_text(case, workdir: Path, dump_steps, threads):
                 lines += [f"energy_model {a} {b} {name}", f"cubic_eps {a} {b} {float(eps[a, b])!r}"]
                 if case.hex_model:
                     lines.append(f"model_eps {a} {b} " + " ".join(repr(float(e)) for e in case.model_eps()[a, b]))
+    mm = case.mobility_models()
+    if mm is not None:
+        for a in range(P):
+            for b in range(a, P):
+                if mm[a, b]:
+                    lines.append(f"mobility_model {a} {b} {case.mobility_model}")
+                    lines.append(f"mobility_eps {a} {b} " + " ".join(repr(float(e)) for e in case.mobility_eps))
     if P > 1:
         f = workdir / "grain_phase.bin"
         case.grain_phase().astype(np.int32).tofile(f)

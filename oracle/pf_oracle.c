@@ -38,6 +38,8 @@ struct op_sim {
     double* facets;               /* FACETED rows: unit facet normal (3), SigmaF, EpsilonEF      */
     int* facet_lo; int* facet_hi; /* [P*P] rows of each pair                                     */
     double* phase_e; double* phase_maxe;   /* [P*P] FACETED Energy (mean SigmaF), MaxEnergy      */
+    int* mobility_model;          /* [P*P]                                                       */
+    double* mobility_eps;         /* [P*P*4]                                                     */
     double* rot;                  /* [G*9] grain RotationMatrix, row-major                       */
     double* quat;                 /* [G*4] grain Orientation (s, x, y, z) as given               */
     int aniso;                    /* some phase pair uses an anisotropic energy model            */
@@ -171,6 +173,14 @@ op_sim* op_create(const op_params* p, int cap)
     s->energy_model = (int*)calloc((size_t)P*P, sizeof(int));
     s->cubic_eps = (double*)calloc((size_t)P*P, sizeof(double));
     s->model_eps = (double*)calloc((size_t)P*P*3, sizeof(double));
+    s->mobility_model = (int*)calloc((size_t)P*P, sizeof(int));
+    s->mobility_eps = (double*)calloc((size_t)P*P*4, sizeof(double));
+    for (int q = 0; q < P*P; q++)
+    {
+        if (p->mobility_model) s->mobility_model[q] = p->mobility_model[q];
+        if (p->mobility_eps) for (int k = 0; k < 4; k++) s->mobility_eps[4*q + k] = p->mobility_eps[4*q + k];
+        if (s->mobility_model[q] != OP_ENERGY_ISO) s->aniso = 1;
+    }
     if (p->model_eps) memcpy(s->model_eps, p->model_eps, (size_t)P*P*3*sizeof(double));
     /* ReadInputFaceted (InterfaceEnergyModel.h:196-246): facet normals (families expanded), Energy
      * = mean SigmaF accumulated in facet order, MaxEnergy = max SigmaF */
@@ -301,6 +311,7 @@ void op_destroy(op_sim* s)
     free(s->pair_sigma); free(s->pair_mu); free(s->dg);
     free(s->energy_model); free(s->cubic_eps); free(s->model_eps); free(s->rot); free(s->quat);
     free(s->facets); free(s->facet_lo); free(s->facet_hi); free(s->phase_e); free(s->phase_maxe);
+    free(s->mobility_model); free(s->mobility_eps);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
     free(s->exist); free(s->stage);
@@ -526,6 +537,59 @@ static double voxel_energy(const op_sim* s, const entry* L, int a, int b)
     return loc;
 }
 
+/* InterfaceMobilityModel::Calculate (include/InterfaceProperties/InterfaceMobilityModel.h:210-265)
+ * for CUBIC, HEXBOETTGER, HEXSUN, HEXYANG, in the reference's operation order. */
+static double mobility_model(const op_sim* s, int q, const double n[3])
+{
+    const double M = s->mu_phase[q];
+    const double* e = s->mobility_eps + 4*q;
+    const double x = n[0], y = n[1], z = n[2];
+    switch (s->mobility_model[q])
+    {
+        case OP_ENERGY_HEXBOETTGER:
+            return M*(1.0 + e[0]*(pow(x, 6) - pow(y, 6) - 15.0*pow(x, 4)*y*y + 15.0*pow(y, 4)*x*x
+                                  + (5.0*pow(z, 4) - 5.0*pow(z, 2) + pow(z, 6))));
+        case OP_ENERGY_HEXSUN:
+            return M*(1.0 - e[0]*sqrt(5.0/16.0/OP_PI)*(3.0*z*z - 1.0)
+                      - e[1]*3.0/16.0/sqrt(OP_PI)*(35.0*pow(z, 4) - 30.0*z*z + 3.0)
+                      - e[2]*sqrt(13.0/OP_PI)/32.0*(231.0*pow(z, 6) - 315.0*pow(z, 4) + 105.0*z*z - 5.0)
+                      - e[3]*sqrt(6006.0/OP_PI)/64.0*(pow(x, 6) - 15.0*pow(x, 4)*y*y + 15.0*x*x*pow(y, 4) - pow(y, 6)));
+        case OP_ENERGY_HEXYANG:
+            return M*(1.0 - e[0]*pow((3.0*z*z - 1.0), 2) - e[1]*pow((x*x*x - 3.0*x*y*y), 2)*pow((9.0*z*z - 1.0 + e[2]), 2));
+        default:   /* CUBIC */
+            return M*(1.0 - e[0]*(1.5 - 2.5*(pow(x, 4) + pow(y, 4) + pow(z, 4))));
+    }
+}
+
+/* The mobility InterfaceProperties::SetSR (src/InterfaceProperties.cpp:680-707) stores for the pair
+ * of list entries a < b: ISO (or the per-grain-pair table) as ip_mobility; an anisotropic model is
+ * summed over the solid grains whose value is neither 0 nor 1, Mobility when there is none. */
+static double voxel_mobility(const op_sim* s, const entry* L, int a, int b)
+{
+    const int ga = L[a].idx, gb = L[b].idx;
+    const int pA = s->grain_phase[ga], pB = s->grain_phase[gb];
+    const int q = pA*s->p.nphases + pB;
+    if (s->mobility_model[q] == OP_ENERGY_ISO) return ip_mobility(s, ga, gb);
+    double loc = 0.0;
+    int solids = 0;
+    if (s->phase_solid[pA] && L[a].val != 0.0 && L[a].val != 1.0)
+    {
+        double n[3];
+        interface_orientation(s, &L[a], n);
+        loc += mobility_model(s, q, n);
+        solids++;
+    }
+    if (s->phase_solid[pB] && L[b].val != 0.0 && L[b].val != 1.0)
+    {
+        double n[3];
+        interface_orientation(s, &L[b], n);
+        loc += mobility_model(s, q, n);
+        solids++;
+    }
+    if (solids == 0) loc = s->mu_phase[q];
+    return loc;
+}
+
 /* PhaseField::LocalN (include/PhaseField.h:84-95) */
 static double local_n(const op_sim* s, const entry* L, int n)
 {
@@ -585,7 +649,7 @@ static int do_increments(const op_sim* s, const entry* L, int n, pair* P)
                                *(L[a].val*L[c].val - L[b].val*L[c].val);
             }
         }
-        dPhi_dt *= ip_mobility(s, ga, gb)*norm_1*scale;
+        dPhi_dt *= (s->aniso ? voxel_mobility(s, L, a, b) : ip_mobility(s, ga, gb))*norm_1*scale;
         /* NodeAB::add_asym1 on an empty FieldsDot creates the entry (NodeAB.h:467-490) */
         P[np].a = a; P[np].b = b; P[np].v1 = dPhi_dt; P[np].alive = 1;
         np++;
@@ -616,7 +680,7 @@ static void df_merge(const op_sim* s, const entry* L, int n, pair* P)
             allowedDG *= s->p.regularization;
             locdG = allowedDG*tanh(locdG/allowedDG);
         }
-        const double dPsi_dt = locdG*ip_mobility(s, ga, gb)*norm*Prefactor;
+        const double dPsi_dt = locdG*(s->aniso ? voxel_mobility(s, L, a, b) : ip_mobility(s, ga, gb))*norm*Prefactor;
         P[pair_pos(a, b, n)].v1 += dPsi_dt;
     }
 }

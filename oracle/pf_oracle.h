@@ -48,6 +48,8 @@ typedef struct op_params {
     const int* facet_start;           /* [P*P+1] FACETED: facets of pair q in facet_data rows    */
     const double* facet_data;         /* rows of h, k, l, SigmaF, EpsilonEF                       */
     const int* facet_family;          /* [P*P] 1: facets stand for their families                */
+    const int* mobility_model;        /* [P*P] 0 ISO, 1 CUBIC, 3..5 HEX* (NULL: all ISO)         */
+    const double* mobility_eps;       /* [P*P*4] its Epsilon1..4                                  */
     const double* quat;               /* [G*4] grain orientation quaternions (w,x,y,z) or NULL  */
     const double* pair_sigma;         /* [G*G] per-grain-pair sigma overriding the phase value, or NULL */
     const double* pair_mu;            /* [G*G] per-grain-pair mobility, or NULL                 */

@@ -60,6 +60,8 @@ struct Case
     std::map<std::pair<int,int>, std::vector<double>> model_eps;   // Epsilon2..4 of the HEX models
     std::map<std::pair<int,int>, std::vector<std::vector<double>>> facets;   // FACETED: h k l SigmaF EpsilonEF
     std::map<std::pair<int,int>, int> facet_family;
+    std::map<std::pair<int,int>, std::string> mobility_model;
+    std::map<std::pair<int,int>, std::vector<double>> mobility_eps;
     std::map<std::pair<int,int>, std::string> energy_model;
     int ngrains = 0;
     std::vector<int> grain_phase;
@@ -121,6 +123,8 @@ static Case parse_case(const std::string& path)
         else if (key == "limit") { int a, b; double v; is >> a >> b >> v; c.limit[{a,b}] = v; }
         else if (key == "energy_model") { int a, b; std::string m; is >> a >> b >> m; c.energy_model[{a,b}] = m; }
         else if (key == "cubic_eps") { int a, b; double v; is >> a >> b >> v; c.cubic_eps[{a,b}] = v; }
+        else if (key == "mobility_model") { int a, b; std::string m; is >> a >> b >> m; c.mobility_model[{a,b}] = m; }
+        else if (key == "mobility_eps") { int a, b; std::vector<double> e(4); is >> a >> b >> e[0] >> e[1] >> e[2] >> e[3]; c.mobility_eps[{a,b}] = e; }
         else if (key == "facet_family") { int a, b, f; is >> a >> b >> f; c.facet_family[{a,b}] = f; }
         else if (key == "facet") { int a, b; std::vector<double> f(5); is >> a >> b >> f[0] >> f[1] >> f[2] >> f[3] >> f[4]; c.facets[{a,b}].push_back(f); }
         else if (key == "model_eps") { int a, b; double e2, e3, e4; is >> a >> b >> e2 >> e3 >> e4; c.model_eps[{a,b}] = {e2, e3, e4}; }
@@ -197,7 +201,16 @@ static void write_opi(const Case& c, const std::string& path)
         if (model == "HEXYANG")
             o << "$EpsilonE1_" << ab << " : " << e1 << "\n" << "$EpsilonE2_" << ab << " : " << ex[0] << "\n"
               << "$EpsilonE3_" << ab << " : " << ex[1] << "\n";
-        o << "$MobilityModel_" << a << "_" << b << " : ISO\n";
+        const std::string mmodel = c.mobility_model.count({a,b}) ? c.mobility_model.at({a,b}) : "ISO";
+        const std::vector<double> me = c.mobility_eps.count({a,b}) ? c.mobility_eps.at({a,b}) : std::vector<double>(4, 0.0);
+        o << "$MobilityModel_" << a << "_" << b << " : " << mmodel << "\n";
+        if (mmodel == "CUBIC" or mmodel == "HEXBOETTGER") o << "$EpsilonM_" << ab << " : " << me[0] << "\n";
+        if (mmodel == "HEXSUN")
+            o << "$EpsilonM20_" << ab << " : " << me[0] << "\n" << "$EpsilonM40_" << ab << " : " << me[1] << "\n"
+              << "$EpsilonM60_" << ab << " : " << me[2] << "\n" << "$EpsilonM66_" << ab << " : " << me[3] << "\n";
+        if (mmodel == "HEXYANG")
+            o << "$EpsilonM1_" << ab << " : " << me[0] << "\n" << "$EpsilonM2_" << ab << " : " << me[1] << "\n"
+              << "$EpsilonM3_" << ab << " : " << me[2] << "\n";
         o << "$Mu_" << a << "_" << b << " : " << m << "\n";
     }
     o << "$TripleJunctionModel : MODEL\n";

@@ -53,6 +53,32 @@ GOLDEN_CASES = {
                                phase_solid=(0, 1), phase_cubic_eps=((0.0, -0.03), (-0.03, 0.0)),
                                phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
                                hex_model="HEXYANG", hex_eps=(0.1, 0.2, 0.0), name="hexyang_nuclei_24"), [1, 30]),
+    # anisotropic interface mobility (CUBIC, HEX*) on the solid-liquid pairs, each with the
+    # matching energy model
+    "mobility_cubic_24": (Case(24, 24, 24, 7, seed=8, iwidth=5.0, dt=0.05, sigma=1.2,
+                               phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                               phase_solid=(0, 1), phase_cubic_eps=((0.0, 0.02), (0.02, 0.0)),
+                               phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                               mobility_model="CUBIC", mobility_eps=(0.2, 0.0, 0.0, 0.0),
+                               name="mobility_cubic_24"), [1, 30]),
+    "mobility_hexboettger_24": (Case(24, 24, 24, 7, seed=9, iwidth=5.0, dt=0.05, sigma=1.2,
+                                     phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                                     phase_solid=(0, 1), phase_cubic_eps=((0.0, 0.05), (0.05, 0.0)),
+                                     phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                                     hex_model="HEXBOETTGER", mobility_model="HEXBOETTGER",
+                                     mobility_eps=(0.15, 0.0, 0.0, 0.0), name="mobility_hexboettger_24"), [1, 30]),
+    "mobility_hexsun_24": (Case(24, 24, 24, 7, seed=10, iwidth=5.0, dt=0.05, sigma=1.2,
+                                phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                                phase_solid=(0, 1), phase_cubic_eps=((0.0, -0.03), (-0.03, 0.0)),
+                                phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                                hex_model="HEXSUN", hex_eps=(0.01, 0.002, 0.004), mobility_model="HEXSUN",
+                                mobility_eps=(-0.05, 0.02, 0.01, 0.005), name="mobility_hexsun_24"), [1, 30]),
+    "mobility_hexyang_24": (Case(24, 24, 24, 7, seed=11, iwidth=5.0, dt=0.05, sigma=1.2,
+                                 phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                                 phase_solid=(0, 1), phase_cubic_eps=((0.0, -0.03), (-0.03, 0.0)),
+                                 phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                                 hex_model="HEXYANG", hex_eps=(0.1, 0.2, 0.0), mobility_model="HEXYANG",
+                                 mobility_eps=(-0.04, 0.1, 0.2, 0.0), name="mobility_hexyang_24"), [1, 30]),
     # FACETED energy model ({100} and {111} facet families) on the solid-liquid pairs
     "faceted_nuclei_24": (Case(24, 24, 24, 7, seed=7, iwidth=5.0, dt=0.05, sigma=1.2,
                                phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
