@@ -6,10 +6,16 @@
 Workload: 256^3 periodic grain growth with driving force -- 2000 seeded Voronoi grains, eta = 6 dx,
 per-grain-pair sigma ~ U[0.8, 1.2], mu = 1, per-grain dG ~ U[0, 0.05], D3Q27 (LB) Laplacian,
 dt = 0.08 (synthetic, seeded; the grid does not fit any public dataset).  One "step" is one full
-time step of the grid.  `value` is voxel-updates/s of the FP32 form with the state resident in
-HBM; the FP64 form (the parity drop-in) is measured the same way and reported under "fp64".
-`e2e` is the same metric through the C ABI from pinned host buffers: upload of the initial state,
-per step the driving-force upload and the grain-volume download, and the final state download.
+time step of the grid; W untimed steps from the Voronoi start, then K timed steps (steps W+1..W+K).
+
+`value` is voxel-updates/s of the FP64 form (the parity drop-in, the reference's own precision)
+with the state resident in HBM; `e2e` is the same metric through the C ABI from pinned host
+buffers: upload of the initial state, per step the driving-force upload and the grain-volume
+download, and the final state download.  The FP32 form is measured the same way under "fp32",
+with its error against the FP64 form after the same W+K steps ("fp32.error").
+
+`--impl reference` times the reference's own OpenMP implementation (oracle/_ref, OpenPhase built
+from its sources) on all host threads over the same step window W+1..W+K.
 
 Multi-GPU (torchrun, one rank per GPU): the grid is cut into x-slabs, one per rank, with an NCCL
 halo-plane exchange and an all-reduce of the grain volumes every step (strong scaling of the same
@@ -125,8 +131,9 @@ def build_inputs(case, threads=0):
     return state, sigma, dg, time.time() - t
 
 
-def device_run(case, precision, k_slots, steps, warmup, device, state, sigma, dg, dist):
-    """Device-resident throughput: W warm-up steps, then exactly K timed steps."""
+def device_run(case, precision, k_slots, steps, warmup, device, state, sigma, dg, dist, keep_final=False):
+    """Device-resident throughput: W warm-up steps, then exactly K timed steps.  keep_final: also
+    return the final state and grain volumes (downloaded after the clock stopped)."""
     import torch
     from openphase_b200.context import Context
 
@@ -162,8 +169,9 @@ def device_run(case, precision, k_slots, steps, warmup, device, state, sigma, dg
     entries_in = s1["entries_in_total"] - s0["entries_in_total"]
     entries_out = s1["entries_out_total"] - s0["entries_out_total"]
     wide = s1["wide_total"] - s0["wide_total"]
+    final = (ctx.download(), ctx.grains()["volume"]) if keep_final else None
     ctx.close()
-    return {
+    return {"final": final,
         "elapsed_ms": elapsed_ms, "kernel_ms": s1["timed_kernel_ms"], "timed_steps": s1["timed_launches"],
         "classify_ms": s1["timed_classify_ms"], "gpu_launches": s1["kernel_launches"] - s0["kernel_launches"],
         "entries_in": entries_in, "entries_out": entries_out, "wide": wide, "status": status | s1["status"],
@@ -283,13 +291,32 @@ def adjoint_run(device):
             "status": int(R.adjoint_status)}
 
 
+def host_cpu():
+    """CPU model, logical and physical core counts of this host."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        import psutil
+        physical = psutil.cpu_count(logical=False)
+    except Exception:  # noqa: BLE001 - reported as unknown
+        physical = None
+    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "physical_cores": physical}
+
+
 def reference_steps(case, state, warmup, steps, threads):
     """Time the reference's own CPU implementation (oracle/_ref, built from the reference sources)
-    on the host cores: returns per-step seconds of the timed steps and the thread count."""
+    on the host cores: warmup + steps full-grid steps from the same initial state, per-step seconds
+    of the last `steps` (omp_get_wtime around each step of the reference driver), thread count."""
     from oracle.bridge import reference_available, run_reference
     if not reference_available():
         return None
-    res, stats = run_reference(case.with_(nsteps=warmup + steps), *state, [warmup + steps], threads=threads)
+    res, stats = run_reference(case, *state, [], threads=threads, nsteps=warmup + steps, proc_bind="close")
     per_step = stats["step_seconds"]
     per_step = per_step if isinstance(per_step, list) else [per_step]
     return per_step[warmup:warmup + steps], int(stats["threads"])
@@ -307,7 +334,7 @@ def oracle_port_steps(case, state, warmup, steps, threads):
     return out, threads
 
 
-def cpu_baseline(case, state, threads, steps=2, warmup=1):
+def cpu_timing(case, state, warmup, steps, threads):
     r = reference_steps(case, state, warmup, steps, threads)
     kind = "reference"
     if r is None:
@@ -315,34 +342,46 @@ def cpu_baseline(case, state, threads, steps=2, warmup=1):
         kind = "port"
     per_step, cores = r
     value = case.n * len(per_step) / sum(per_step)
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{len(per_step)} timed full-grid steps after {warmup} warm-up step(s) of the same "
-                      f"{case.nx}^3 workload, OpenMP on {cores} host threads"}
+    info = host_cpu()
+    return value, per_step, {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "omp_proc_bind": "close", **info}
 
 
-def run_reference_arm(args, case, rank):
+def cpu_baseline(case, state, threads, warmup, steps=3):
+    """A bounded sample (about half a minute of host time): the first `steps` steps of the GPU's
+    timed window (steps warmup+1 ..), after the same `warmup` steps."""
+    value, per_step, d = cpu_timing(case, state, warmup, steps, threads)
+    d["sample"] = (f"steps {warmup + 1}-{warmup + len(per_step)} (the first {len(per_step)} of the timed window) "
+                   f"of the same {case.nx}^3 workload after {warmup} untimed steps, OpenMP on {d['cores']} "
+                   f"host threads")
+    return d
+
+
+def workload_config(case, k_slots, world):
+    """The `config` object of both arms' lines."""
+    return {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains,
+            "eta_cells": case.iwidth, "dt": case.dt, "stencil": "D3Q27 (LB)", "k_slots": k_slots,
+            "parallelism": f"x-slabs x{world} (NCCL halo exchange + volume all-reduce)" if world > 1
+            else "single GPU",
+            "l2": "inputs larger than L2 (the K-slot state is >126 MB)"}
+
+
+def run_reference_arm(args, case, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     state, sigma, dg, _ = build_inputs(case, threads)
-    # a bounded sample of the workload: full-grid reference steps, capped so the arm ends in minutes
-    warm = min(args.warmup, 1)
-    k = max(1, min(args.steps, 6))
-    r = reference_steps(case, state, warm, k, threads)
-    kind = "reference"
-    if r is None:
-        r = oracle_port_steps(case, state, warm, k, threads)
-        kind = "port"
-    per_step, cores = r
-    value = case.n * len(per_step) / sum(per_step)
+    # the same window as the GPU arm: W untimed steps, then K timed steps
+    value, per_step, cpu = cpu_timing(case, state, args.warmup, args.steps, threads)
+    cpu["sample"] = (f"steps {args.warmup + 1}-{args.warmup + len(per_step)} of the workload after "
+                     f"{args.warmup} untimed steps (the GPU arm's timed window), OpenMP on {cpu['cores']} "
+                     f"host threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": len(per_step), "warmup": warm, "ms_per_step": 1e3 * sum(per_step) / len(per_step),
+        "steps": len(per_step), "warmup": args.warmup, "ms_per_step": 1e3 * sum(per_step) / len(per_step),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{len(per_step)} full-grid steps after {warm} warm-up step(s), "
-                                   f"OpenMP on {cores} host threads"},
+        "config": workload_config(case, args.k_slots, world),
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -359,6 +398,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-fp32-error", action="store_true")
     ap.add_argument("--workload", default="grain_growth_dg_256")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -372,7 +412,7 @@ def main():
     local_rank = _env_int("LOCAL_RANK", 0)
 
     if args.impl == "reference":
-        return run_reference_arm(args, case, rank)
+        return run_reference_arm(args, case, rank, world)
 
     import torch
     torch.cuda.set_device(local_rank)
@@ -387,13 +427,13 @@ def main():
     state, sigma, dg, t_init = build_inputs(case, threads)
 
     runs = {}
-    for precision in ("fp32", "fp64"):
+    for precision in ("fp64", "fp32"):
         if world > 1:
             runs[precision] = slab_run(case, precision, args.k_slots, args.steps, args.warmup, local_rank,
                                        state, sigma, dg, dist)
         else:
             runs[precision] = device_run(case, precision, args.k_slots, args.steps, args.warmup, local_rank,
-                                         state, sigma, dg, dist)
+                                         state, sigma, dg, dist, keep_final=not args.no_fp32_error)
 
     def agg(ms):
         t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
@@ -427,6 +467,8 @@ def main():
                          "kernel": "step: tile_classify_kernel + bucket_scan_kernel + list_compute_kernel<N=2..8> + warp_general_kernel + grains_update_kernel",
                          "kernel_ms": kernel_ms, "classify_ms": classify_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "algorithmic_bytes_rule": "|W| * 2 * (1 + 8*(2+s)) + N^3 (K = 8 slot records; the run stores K = "
+                                                   f"{args.k_slots} slots but touches only the ones a voxel holds)",
                          "sparse_bytes_per_launch": sparse_bytes,
                          "sparse_achieved": sparse_bytes / (kernel_ms / 1e3) / 1e9,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
@@ -434,12 +476,26 @@ def main():
             "wide_fraction": r["wide"] / (case.n * args.steps),
         }
 
-    e2e = None
+    fp32_error = None
+    if runs["fp64"].get("final") and runs["fp32"].get("final"):
+        from openphase_b200.compare import precision_error
+        (st64, v64), (st32, v32) = runs["fp64"]["final"], runs["fp32"]["final"]
+        fp32_error = precision_error(st32, v32, st64, v64, case.ngrains)
+        fp32_error["after_steps"] = args.warmup + args.steps
+        fp32_error["against"] = "FP64 form of this library from the same initial state (the FP64 form matches the reference)"
+        fp32_error["bar"] = {"max_dphi": 1e-4, "volume_rel_max": 1e-3,
+                             "met": bool(fp32_error["max_dphi"] <= 1e-4 and fp32_error["volume_rel_max"] <= 1e-3)}
+        for r in runs.values():
+            r["final"] = None
+
+    e2e = {}
     if not args.no_e2e and world == 1:
-        er = e2e_run(case, "fp32", args.k_slots, args.steps, local_rank, state, sigma, dg)
-        sec = agg(er["seconds"] * 1e3) / 1e3
-        e2e = {"value": world * case.n * args.steps / sec, "unit": UNIT,
-               "h2d_bytes_per_step": int(er["h2d_per_step"]), "d2h_bytes_per_step": int(er["d2h_per_step"])}
+        for precision in ("fp64", "fp32"):
+            er = e2e_run(case, precision, args.k_slots, args.steps, local_rank, state, sigma, dg)
+            sec = agg(er["seconds"] * 1e3) / 1e3
+            e2e[precision] = {"value": world * case.n * args.steps / sec, "unit": UNIT,
+                              "h2d_bytes_per_step": int(er["h2d_per_step"]),
+                              "d2h_bytes_per_step": int(er["d2h_per_step"])}
 
     adjoint = None
     if not args.no_adjoint and world == 1:
@@ -447,7 +503,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(case, state, os.cpu_count() or 1)
+        cpu = cpu_baseline(case, state, os.cpu_count() or 1, args.warmup)
 
     if dist is not None:
         dist.barrier()
@@ -456,27 +512,24 @@ def main():
         return 0
     f32, f64 = out["fp32"], out["fp64"]
     line = {
-        "metric": METRIC, "value": f32["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": f32["ms_per_step"], "higher_is_better": True,
+        "metric": METRIC, "value": f64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": f64["ms_per_step"], "higher_is_better": True,
         "scaling": "strong" if world > 1 else "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains,
-                   "eta_cells": case.iwidth, "dt": case.dt, "stencil": "D3Q27 (LB)", "k_slots": args.k_slots,
-                   "parallelism": f"x-slabs x{world} (NCCL halo exchange + volume all-reduce)" if world > 1
-                   else "single GPU",
-                   "l2": "inputs larger than L2 (the K-slot state is >126 MB)",
-                   "initial_state_seconds": round(t_init, 2)},
-        "clocks": f32["clocks"],
-        "e2e": e2e,
-        "gpu_launches": f32["gpu_launches"],
-        "roofline": f32["roofline"],
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(case, args.k_slots, world),
+        "clocks": f64["clocks"],
+        "e2e": e2e.get("fp64"),
+        "gpu_launches": f64["gpu_launches"],
+        "roofline": f64["roofline"],
         "cpu_baseline": cpu,
-        "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "roofline": f64["roofline"],
-                 "clocks": f64["clocks"], "status": f64["status"]},
+        "fp32": {"value": f32["value"], "ms_per_step": f32["ms_per_step"], "e2e": e2e.get("fp32"),
+                 "roofline": f32["roofline"], "clocks": f32["clocks"], "status": f32["status"],
+                 "gpu_launches": f32["gpu_launches"], "error": fp32_error},
         "fp32_over_fp64": f32["value"] / f64["value"],
         "adjoint": adjoint,
         "status": {"fp32": f32["status"], "fp64": f64["status"]},
-        "wide_fraction": f32["wide_fraction"],
+        "wide_fraction": f64["wide_fraction"],
+        "initial_state_seconds": round(t_init, 2),
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -67,6 +67,8 @@ struct opgpu_ctx {
     std::vector<int16_t> h_gphase;      // [G] phase of every grain
     std::vector<double> h_quat;         // [G*4] orientations (s, x, y, z) as given; empty: unrotated
     std::vector<double> h_user_sigma;   // [G*G] energies given to opgpu_set_pair_table; empty: none
+    std::vector<double> h_dg;           // [G] driving forces given to opgpu_set_driving_force
+    std::vector<double> h_dg_pair;      // [G*G] host side of the limited driving-force table
     bool pair_energy_dirty = true;
     uint32_t* d_status = nullptr;
     unsigned long long* d_counters = nullptr;
@@ -785,8 +787,15 @@ extern "C" uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG)
     if (!ctx->d_dg) CK(dalloc(&ctx->d_dg, ctx->G));
     CK(cudaMemcpyAsync(ctx->d_dg, dG, ctx->G * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    // the pair table is rebuilt only when the forces change (or with the model and the grains)
+    const bool same = ctx->sp.use_dg && ctx->h_dg.size() == (size_t)ctx->G &&
+                      std::memcmp(ctx->h_dg.data(), dG, ctx->G * sizeof(double)) == 0;
+    if (!same)
+    {
+        ctx->h_dg.assign(dG, dG + ctx->G);
+        ctx->dg_pair_dirty = true;
+    }
     ctx->sp.use_dg = 1;
-    ctx->dg_pair_dirty = true;
     return OPGPU_OK;
 }
 
@@ -861,6 +870,43 @@ uint32_t refresh_pair_energy(opgpu_ctx* ctx)
     CK(cudaMemcpy(ctx->d_pair_sigma, tab.data(), GG * sizeof(double), cudaMemcpyHostToDevice));
     ctx->sp.pair_mode = OPGPU_PAIRS_TABLE;
     ctx->pair_energy_dirty = false;
+    return OPGPU_OK;
+}
+
+// The tanh-limited driving force of every grain pair, allowed*tanh((dG_b - dG_a)/allowed) with
+// allowed = Limit*Prefactor*MaxEnergy*RegularizationFactor (src/DrivingForce.cpp:548-583).  It
+// depends on the pair only, so it is tabulated (G*G) whenever the forces or the model change, on
+// the host with the C library's tanh: the function the reference evaluates per voxel, so that the
+// step's values equal the reference's bit for bit (CUDA's tanh differs from it in the last bit for
+// some arguments, which can tip a threshold decision of the step).
+uint32_t build_dg_pair(opgpu_ctx* ctx)
+{
+    if (!(ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && ctx->dg_pair_dirty)) return OPGPU_OK;
+    if (ctx->h_dg.size() != (size_t)ctx->G || ctx->h_gphase.size() != (size_t)ctx->G)
+        return fail(ctx, OPGPU_E_STATE, "driving-force table: grains and driving forces out of step");
+    const int G = ctx->G, P = ctx->sp.nphases;
+    const size_t GG = (size_t)G * G;
+    if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, GG));
+    ctx->h_dg_pair.resize(GG);
+    const double* dg = ctx->h_dg.data();
+    const int16_t* ph = ctx->h_gphase.data();
+    const StepParams& sp = ctx->sp;
+    double* out = ctx->h_dg_pair.data();
+#pragma omp parallel for schedule(static)
+    for (int a = 0; a < G; a++)
+        for (int b = 0; b < G; b++)
+        {
+            double locdG = dg[b] - dg[a];
+            if (sp.limiting)
+            {
+                const double allowed = sp.allowed_p[ph[a] * P + ph[b]];
+                locdG = allowed * std::tanh(locdG / allowed);
+            }
+            out[(size_t)a * G + b] = locdG;
+        }
+    // pageable source: the call returns once the table is staged, the host copy stays valid
+    CK(cudaMemcpyAsync(ctx->d_dg_pair, out, GG * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->dg_pair_dirty = false;
     return OPGPU_OK;
 }
 
@@ -1007,14 +1053,7 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
     StepParams sp = ctx->sp;
     sp.dt = dt;
     const bool pair_table = sp.use_dg && ctx->G <= kMaxPairTableGrains;
-    if (pair_table && ctx->dg_pair_dirty)
-    {
-        if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, (size_t)ctx->G * ctx->G));
-        const int rc = launch_dg_pair(sp, ctx->d_dg, ctx->d_gphase, ctx->d_dg_pair, ctx->stream);
-        ctx->kernel_launches++;
-        if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("driving-force table: ") + cudaGetErrorString((cudaError_t)rc));
-        ctx->dg_pair_dirty = false;
-    }
+    if (uint32_t r = build_dg_pair(ctx)) return r;
     for (int s = 0; s < nsteps; s++)
     {
         const int in = ctx->cur, out = 1 - ctx->cur;
@@ -1349,15 +1388,7 @@ uint32_t copy_grains(opgpu_ctx* ctx, double* vol, double* mx, double* vr, int8_t
 uint32_t refresh_dg_pair(opgpu_ctx* ctx)
 {
     if (uint32_t r = refresh_pair_energy(ctx)) return r;
-    if (ctx->sp.use_dg && ctx->G <= kMaxPairTableGrains && ctx->dg_pair_dirty)
-    {
-        if (!ctx->d_dg_pair) CK(dalloc(&ctx->d_dg_pair, (size_t)ctx->G * ctx->G));
-        const int rc = launch_dg_pair(ctx->sp, ctx->d_dg, ctx->d_gphase, ctx->d_dg_pair, ctx->stream);
-        if (rc != 0) return fail(ctx, OPGPU_E_CUDA, "driving-force table");
-        ctx->kernel_launches++;
-        ctx->dg_pair_dirty = false;
-    }
-    return OPGPU_OK;
+    return build_dg_pair(ctx);
 }
 
 uint32_t ensure_adjoint(opgpu_ctx* ctx)

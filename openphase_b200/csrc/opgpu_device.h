@@ -168,9 +168,6 @@ int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int v
 // The classify kernel of the tiled step alone; returns the number of classify blocks or < 0.
 int launch_classify_f64(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
 int launch_classify_f32(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
-// Fill out[a*G+b] with the limited driving force of every grain pair (defined in step_f64.cu, so
-// that it is compiled exactly like the in-place evaluation of the FP64 form).
-int launch_dg_pair(const StepParams& p, const double* dg, const int16_t* gphase, double* out, void* stream);
 // Add the volumes of the window planes of a state to vol_acc (defined in step_f64.cu).
 int launch_volume_recount(const StepParams& p, const uint8_t* cnt, const int16_t* idx, const void* val, int fp32,
                           double* vol_acc, void* stream);

@@ -15,22 +15,6 @@ int launch_classify_f64(const StepParams& p, const StepArrays& a, int k_slots, v
     return launch_classify<double>(p, a, k_slots, stream);
 }
 
-__global__ void dg_pair_kernel(const __grid_constant__ StepParams p, const double* __restrict__ dg,
-                               const int16_t* __restrict__ gphase, double* __restrict__ out)
-{
-    const long long G = p.ngrains;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= G * G) return;
-    const int ga = (int)(i / G), gb = (int)(i % G);
-    double locdG = dg[gb] - dg[ga];
-    if (p.limiting)
-    {
-        const double allowed = p.allowed_p[gphase[ga] * p.nphases + gphase[gb]];
-        locdG = allowed * tanh(locdG / allowed);
-    }
-    out[i] = locdG;
-}
-
 // Grain volumes of the window planes of a state (slab decomposition: before the first step).
 __global__ void volume_recount_kernel(const __grid_constant__ StepParams p, const uint8_t* __restrict__ cnt,
                                       const int16_t* __restrict__ idx, const void* __restrict__ val, int fp32,
@@ -62,13 +46,6 @@ int launch_volume_recount(const StepParams& p, const uint8_t* cnt, const int16_t
 {
     volume_recount_kernel<<<(unsigned)((p.n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         p, cnt, idx, val, fp32, vol_acc);
-    return (int)cudaGetLastError();
-}
-
-int launch_dg_pair(const StepParams& p, const double* dg, const int16_t* gphase, double* out, void* stream)
-{
-    const long long GG = (long long)p.ngrains * p.ngrains;
-    dg_pair_kernel<<<(unsigned)((GG + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, dg, gphase, out);
     return (int)cudaGetLastError();
 }
 

@@ -70,6 +70,8 @@ def oracle_lib():
         L.op_wide_count.argtypes = [C.c_void_p]
         L.op_get_grains.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         L.op_set_grains.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        L.op_raw_counts.restype = C.c_long
+        L.op_raw_counts.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_void_p]
         _olib = L
     return _olib
 
@@ -190,17 +192,43 @@ def positive_entries(counts, idx, val):
     return new_counts, np.asarray(idx)[keep], np.asarray(val)[keep]
 
 
+def parse_raw(data: bytes):
+    """Parse a raw PhaseField file (the reference's PhaseField::Write) into (dims, counts, idx, val);
+    the per-voxel count walk runs in the oracle library (a Python loop takes minutes at 256^3)."""
+    nx, ny, nz = (int(x) for x in np.frombuffer(data[:12], dtype=np.int32))
+    words = np.frombuffer(data, dtype=np.uint64, offset=12)
+    n = nx * ny * nz
+    counts = np.empty(n, dtype=np.int32)
+    used = oracle_lib().op_raw_counts(_p(words), words.size, n, _p(counts))
+    if used != words.size:
+        raise ValueError("raw file size does not match its counts")
+    starts = np.zeros(n, dtype=np.int64)
+    np.cumsum(1 + 2 * counts[:-1].astype(np.int64), out=starts[1:])
+    total = int(counts.sum(dtype=np.int64))
+    first = np.repeat(starts + 1, counts)
+    rank = np.arange(total, dtype=np.int64) - np.repeat(np.cumsum(counts, dtype=np.int64) - counts, counts)
+    entry_pos = first + 2 * rank
+    idx = words[entry_pos].astype(np.int32)
+    val = words[entry_pos + 1].view(np.float64).copy()
+    return (nx, ny, nz), counts, idx, val
+
+
 def reference_available() -> bool:
     return REF_DRIVER.exists()
 
 
-def _case_text(case, workdir: Path, dump_steps, threads):
+def _case_text(case, workdir: Path, dump_steps, threads, nsteps=None, vtk_steps=(), restart_grains=None):
     P = case.nphases
+    nsteps = max(dump_steps) if nsteps is None else nsteps
     lines = [f"nx {case.nx}", f"ny {case.ny}", f"nz {case.nz}", f"dx {case.dx!r}", f"iwidth {case.iwidth!r}",
-             f"stencil {case.stencil}", f"dt {case.dt!r}", f"nsteps {max(dump_steps)}", f"nphases {P}",
+             f"stencil {case.stencil}", f"dt {case.dt!r}", f"nsteps {nsteps}", f"nphases {P}",
              f"ngrains {case.ngrains}", f"limiting {int(case.limiting)}",
              f"regularization {case.regularization!r}", f"tj_factor {case.tj_factor!r}",
              "dump_steps " + " ".join(str(s) for s in dump_steps)]
+    if vtk_steps:
+        lines.append("vtk_steps " + " ".join(str(s) for s in vtk_steps))
+    if restart_grains:
+        lines.append(f"restart_grains_file {restart_grains}")
     sig, mu, lim, sol = case.sigma_phase(), case.mu_phase(), case.limit_phase(), case.solid_phase()
     eps = case.cubic_eps()
     for a in range(P):
@@ -251,22 +279,32 @@ def _case_text(case, workdir: Path, dump_steps, threads):
     return "\n".join(lines) + "\n"
 
 
-def run_reference(case, counts, idx, val, dump_steps, threads=0, workdir=None):
+def run_reference(case, counts, idx, val, dump_steps, threads=0, workdir=None, nsteps=None, proc_bind="close",
+                  vtk_steps=(), restart_grains=None, keep_files=False):
     """Run the compiled reference on the case; returns {step: (counts, idx, val, volume, volume_ratio)}
-    and the stats dictionary (wall time of the step loop, threads, wide-interface counts)."""
-    from openphase_b200.initializations import raw_bytes, parse_raw
+    and the stats dictionary (wall time of the step loop, threads, wide-interface counts).
+
+    nsteps defaults to the last dump step (dump_steps may then be empty); the OpenMP threads are
+    bound with OMP_PROC_BIND=proc_bind.  vtk_steps: steps at which the reference writes its VTK file
+    (returned as bytes under stats["vtk"][step]); restart_grains: a grain-record file to restart from
+    (the reference's PhaseField::Read + FieldsProperties.Read + Finalize).  Each dumped step also
+    carries the reference's grain-record file bytes under stats["grains_file"][step]."""
+    from openphase_b200.initializations import raw_bytes
 
     if not REF_DRIVER.exists():
         raise FileNotFoundError("reference driver not built (make -C oracle ref)")
     tmp = tempfile.TemporaryDirectory() if workdir is None else None
     wd = Path(workdir or tmp.name)
     wd.mkdir(parents=True, exist_ok=True)
-    (wd / "case.txt").write_text(_case_text(case, wd, dump_steps, threads))
+    (wd / "case.txt").write_text(_case_text(case, wd, dump_steps, threads, nsteps, vtk_steps, restart_grains))
     (wd / "init.dat").write_bytes(raw_bytes(case.nx, case.ny, case.nz, counts, idx, val))
     out = wd / "out"
     out.mkdir(exist_ok=True)
+    env = dict(os.environ)
+    if proc_bind:
+        env["OMP_PROC_BIND"] = proc_bind
     r = subprocess.run([str(REF_DRIVER), str(wd / "case.txt"), str(wd / "init.dat"), str(out)],
-                       capture_output=True, text=True)
+                       capture_output=True, text=True, env=env)
     if r.returncode != 0:
         raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stderr[-2000:]}")
     res = {}
@@ -279,6 +317,12 @@ def run_reference(case, counts, idx, val, dump_steps, threads=0, workdir=None):
     for line in (out / "stats.txt").read_text().splitlines():
         k, *vals = line.split()
         stats[k] = [float(x) for x in vals] if len(vals) > 1 else float(vals[0])
+    stats["vtk"] = {}
+    for st in vtk_steps:
+        files = sorted(out.glob(f"PhaseField_*{st}.vts"))
+        files = [f for f in files if int(f.stem.split("_")[-1]) == st]
+        stats["vtk"][st] = files[0].read_bytes()
+    stats["grains_file"] = {st: (out / f"FP_{st}.dat").read_bytes() for st in dump_steps}
     if tmp is not None:
         tmp.cleanup()
     return res, stats

@@ -1099,3 +1099,21 @@ void op_set_grains(op_sim* s, const double* volume_ratio, const double* max_volu
     if (stage) memcpy(s->stage, stage, G*sizeof(int32_t));
     if (ref_volume) memcpy(s->ref_volume, ref_volume, G*sizeof(double));
 }
+
+/* Per-voxel entry counts of a raw PhaseField file (the format of PhaseField::Write,
+ * src/PhaseField.cpp:2340-2388: after the 3 x int32 header, per voxel a size_t count and that many
+ * (size_t index, double value) pairs).  `words` are the 8-byte words after the header.  Returns the
+ * number of words the n voxels take, or -1 if they run past nwords. */
+long op_raw_counts(const uint64_t* words, long nwords, long n, int32_t* counts)
+{
+    long pos = 0;
+    for (long v = 0; v < n; v++)
+    {
+        if (pos >= nwords) return -1;
+        const uint64_t c = words[pos];
+        if (c > (uint64_t)(nwords - pos - 1) / 2) return -1;
+        counts[v] = (int32_t)c;
+        pos += 1 + 2 * (long)c;
+    }
+    return pos;
+}

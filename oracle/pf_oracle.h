@@ -89,6 +89,10 @@ void    op_get_grains(const op_sim* s, double* volume, double* volume_ratio, dou
 void    op_set_grains(op_sim* s, const double* volume_ratio, const double* max_volume,
                       const int32_t* exist, const int32_t* stage, const double* ref_volume);
 
+/* Per-voxel counts of the n voxel lists of a raw PhaseField file (words after the 12-byte header);
+ * returns the words they take or -1 if nwords is too short. */
+long    op_raw_counts(const uint64_t* words, long nwords, long n, int32_t* counts);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,10 @@
 //     PF_<step>.dat    PhaseField::Write raw state at every requested dump step
 //     V_<step>.bin     per-grain Volume (double[G]) at the same steps
 //     VR_<step>.bin    per-grain VolumeRatio (double[G])
+//     FP_<step>.dat    grain records in the restart format (GrainsProperties::Write)
+//     PhaseField_<step>.vts  PhaseField::WriteVTK output at the vtk_steps
+// With "restart_grains_file" the run starts from the raw state and those grain records followed
+// by PhaseField::Finalize, the reference's restart (src/PhaseField.cpp:2541-2554).
 //     stats.txt        wide-interface voxel count per step, step-loop wall time, threads
 
 #include "Settings.h"
@@ -71,6 +75,8 @@ struct Case
     double tj_factor = 0.0;
     bool consider_nucleus_volume = true;
     std::set<int> dump_steps;
+    std::set<int> vtk_steps;       // PhaseField::WriteVTK at these steps
+    std::string restart_grains;    // FieldsProperties file to restart from (with the raw state)
     int threads = 0;
 };
 
@@ -139,6 +145,8 @@ static Case parse_case(const std::string& path)
         else if (key == "tj_factor") is >> c.tj_factor;
         else if (key == "consider_nucleus_volume") { int v; is >> v; c.consider_nucleus_volume = v != 0; }
         else if (key == "dump_steps") { int s; while (is >> s) c.dump_steps.insert(s); }
+        else if (key == "vtk_steps") { int s; while (is >> s) c.vtk_steps.insert(s); }
+        else if (key == "restart_grains_file") is >> c.restart_grains;
         else if (key == "threads") is >> c.threads;
         else { fprintf(stderr, "ref_driver: unknown key %s\n", key.c_str()); exit(2); }
     }
@@ -249,6 +257,8 @@ static void dump(const Case& c, PhaseField& Phi, const std::string& out, int ste
     }
     write_doubles(out + "/V_" + tag + ".bin", V);
     write_doubles(out + "/VR_" + tag + ".bin", VR);
+    // grain records in the restart format (GrainsProperties::Write, include/GrainsProperties.h:762-792)
+    Phi.FieldsProperties.Write(out + "/FP_" + tag + ".dat");
 }
 
 int main(int argc, char* argv[])
@@ -283,8 +293,20 @@ int main(int argc, char* argv[])
             Phi.FieldsProperties[g].Orientation = Quaternion({q[4*g], q[4*g + 1], q[4*g + 2], q[4*g + 3]});
     }
     if (!Phi.Read(raw_in)) { fprintf(stderr, "ref_driver: Read failed\n"); return 3; }
-    Phi.FinalizeInitialization(BC);
+    if (c.restart_grains.empty())
+    {
+        Phi.FinalizeInitialization(BC);
+    }
+    else
+    {
+        // restart: the raw state plus the grain records, then Finalize
+        // (PhaseField::Read(Settings, BC, tStep), src/PhaseField.cpp:2541-2554)
+        if (!Phi.FieldsProperties.Read(c.restart_grains)) { fprintf(stderr, "ref_driver: grains Read failed\n"); return 3; }
+        Phi.Finalize(BC);
+    }
+    S.VTKDir = out + "/";
     if (c.dump_steps.count(0)) dump(c, Phi, out, 0);
+    if (c.vtk_steps.count(0)) Phi.WriteVTK(S, 0);
 
     const bool use_pair = !c.pair_sigma.empty();
     const bool use_dg   = !c.dg.empty();
@@ -356,6 +378,7 @@ int main(int argc, char* argv[])
         }
         wide[step] = w;
         if (c.dump_steps.count(step)) dump(c, Phi, out, step);
+        if (c.vtk_steps.count(step)) Phi.WriteVTK(S, step);
     }
 
     std::ofstream st(out + "/stats.txt");

@@ -2,7 +2,8 @@
 
 Bar: per-voxel index lists identical (borderline voxels within 1e-12 of the finalize threshold are
 counted and reported), max|dphi| <= 1e-9.  The FP64 form differs from the reference arithmetic only
-in tanh (CUDA vs libm) and in the summation order of the grain volumes.  The volumes feed back into
+in the summation order of the grain volumes (the limited driving force is tabulated per grain pair
+with the C library's tanh, the reference's).  The volumes feed back into
 the kinetics only for grains below the reference volume (VolumeRatio < 1); the strict cases keep all
 grains above it, the small-grain cases are held to the bar for 10 steps and to a mismatch budget
 after that (the reference itself sums the volumes in a thread-schedule-dependent order).
@@ -26,8 +27,7 @@ STRICT = {
     "isotropic_big": Case(48, 40, 32, 8, seed=5, iwidth=5.0, dt=0.1, stencil="ISOTROPIC", name="isotropic_big"),
     "simple_big": Case(48, 40, 32, 8, seed=6, iwidth=5.0, dt=0.1, stencil="SIMPLE", name="simple_big"),
 }
-# per-grain-pair sigma and driving force with large grains: tanh differs between CUDA and libm in the
-# last bits, so the bar holds for 60 steps and borderline decisions are counted after that
+# per-grain-pair sigma and driving force with large grains (VolumeRatio = 1 throughout)
 DRIVEN = {
     "pairs_dg_48": Case(48, 40, 32, 12, seed=8, iwidth=5.0, dt=0.08, sigma=1.2, sigma_pairs=(0.8, 0.4),
                         dg_scale=0.05, name="pairs_dg_48"),
@@ -83,18 +83,16 @@ def test_fp64_matches_oracle_strict(name, variant):
 
 @pytest.mark.parametrize("name", list(DRIVEN))
 def test_fp64_matches_oracle_driven(name):
+    """Per-grain-pair sigma and driving force, large grains: the tanh-limited force of every pair is
+    tabulated with the C library's tanh (the reference's), so the bar holds over all 150 steps."""
     case = DRIVEN[name]
     res = _run_pair(case, [1, 2, 10, 60, 150])
     for s, r in res:
         if s:
             assert r["status_gpu"] & 0b11 == 0, (s, r)
-        if s <= 60:
-            assert r["non_borderline_mismatch_voxels"] == 0, (s, r)
-            assert r["max_dphi"] <= TOL, (s, r)
-        else:
-            # a borderline decision (counted) may seed a local divergence after the strict window
-            assert r["set_mismatch_voxels"] <= 1e-4 * case.n, (s, r)
-            assert r["vol_rel"] <= 1e-6, (s, r)
+            assert r["vol_rel"] <= 1e-12, (s, r)
+        assert r["non_borderline_mismatch_voxels"] == 0, (s, r)
+        assert r["max_dphi"] <= TOL, (s, r)
     print(name, res[-1])
 
 
