@@ -185,10 +185,38 @@ uint32_t opgpu_download_flags(opgpu_ctx* ctx, int8_t* flags);
  * pool, and callers that must not stall other streams (cudaFree waits for all work on the
  * device), e.g. a monitor that reads the flags while steps run on other contexts.
  * Limit: grids of at most 16,777,216 voxels (256^3); larger grids get OPGPU_E_INVALID with a
- * message.  The first call on a device does a one-time set-up (it looks up the scratch address
- * on that device) and should come before any stream capture.  The scratch is shared by all
- * contexts on a device: overlapping calls (from several threads) race, so serialise them. */
+ * message.  The first call on each context does a one-time set-up (it looks up the scratch
+ * address on the context's device) and should come before any stream capture.  The 16 MiB are
+ * taken from device memory when the library's device code is loaded on a device, in every process
+ * that loads the library, not at the call.  The scratch is shared by all contexts on a device:
+ * overlapping calls (from several threads) race, so serialise them. */
 uint32_t opgpu_download_flags_noalloc(opgpu_ctx* ctx, int8_t* flags);
+
+/* Grain records in the reference's restart format: the binary file of GrainsProperties::Write /
+ * Read (include/GrainsProperties.h:762-825, one Grain::Write record per grain, :197-231): size_t G,
+ * then per grain Exist, Mobile, Stage, Parent, Phase, Variant, State, Density, RefVolume, Volume,
+ * MAXVolume, the rigid-body vectors and the orientation quaternion.  Fields this library does not
+ * model are written with the reference's defaults (Mobile true, Parent/Variant 0, Density 0, motion
+ * zero) and ignored when read.  A restart, like PhaseField::Read(Settings, BC, tStep)
+ * (src/PhaseField.cpp:2541-2554: raw state, FieldsProperties.Read, Finalize), is
+ *   opgpu_read_raw -> opgpu_read_grains -> opgpu_finalize_initialization,
+ * the last of which then keeps the MAXVolume read from the file.  opgpu_read_grains needs
+ * opgpu_set_grains with the same grain count first and replaces phases, stages, reference volumes,
+ * volumes, MAXVolume (VolumeRatio = MAXVolume/RefVolume as Grain::Read) and orientations. */
+uint32_t opgpu_write_grains(opgpu_ctx* ctx, const char* path);
+uint32_t opgpu_read_grains(opgpu_ctx* ctx, const char* path);
+/* VTK output of the current state, byte for byte what PhaseField::WriteVTK writes for a single-
+ * resolution grid without curvature output (src/PhaseField.cpp:2128-2150, VTK::Write
+ * src/VTK.cpp:75-95): an ASCII StructuredGrid (.vts) with the point data Interfaces, Flags,
+ * PhaseFields (majority grain), PhaseFraction_<p>, Junctions (list length including the zero-valued
+ * candidates), Variants, ParentGrain, then the point coordinates. */
+uint32_t opgpu_write_vtk(opgpu_ctx* ctx, const char* path);
+/* The same file from ragged host lists (no device needed): counts[N], idx/val of all entries in
+ * voxel order, grain_phase[ngrains] (NULL: all phase 0), the grid's OPGPU_STENCIL_* choices (they
+ * decide which neighbours bring candidates). */
+uint32_t opgpu_write_vtk_host(int32_t nx, int32_t ny, int32_t nz, const int32_t* counts, const int32_t* idx,
+                              const double* val, int32_t ngrains, const int32_t* grain_phase, int32_t nphases,
+                              int32_t laplacian_stencil, int32_t gradient_stencil, const char* path);
 
 /* ---- the time step -------------------------------------------------------------------------- */
 /* nsteps repetitions of the reference step sequence

@@ -102,6 +102,31 @@ public:
         check(opgpu_finalize_initialization(ctx_), "PhaseField::FinalizeInitialization");
         stage_ = Stage::Idle;
     }
+    /* Restart pair of PhaseField::Write(Settings, tStep) / Read(Settings, BC, tStep)
+     * (src/PhaseField.cpp:2390-2402, 2541-2554): the raw state and the grain records
+     * (GrainsProperties::Write / Read, include/GrainsProperties.h:762-825); Read finalizes. */
+    bool WriteRestart(const std::string& RawFileName, const std::string& GrainsFileName)
+    {
+        if (!Write(RawFileName)) return false;
+        const uint32_t st = opgpu_write_grains(ctx_, GrainsFileName.c_str());
+        if (st & OPGPU_E_IO) return false;
+        check(st, "PhaseField::Write");
+        return true;
+    }
+    bool ReadRestart(const BoundaryConditions& BC, const std::string& RawFileName, const std::string& GrainsFileName)
+    {
+        if (!Read(RawFileName)) return false;
+        const uint32_t st = opgpu_read_grains(ctx_, GrainsFileName.c_str());
+        if (st & OPGPU_E_IO) return false;
+        check(st, "PhaseField::Read");
+        FinalizeInitialization(BC);
+        return true;
+    }
+    /* PhaseField::WriteVTK (src/PhaseField.cpp:2128-2150), single resolution, no curvature output. */
+    void WriteVTK(const std::string& FileName)
+    {
+        check(opgpu_write_vtk(ctx_, FileName.c_str()), "PhaseField::WriteVTK");
+    }
     /* PhaseField::NormalizeIncrements (src/PhaseField.cpp:1334-1349). */
     void NormalizeIncrements(const BoundaryConditions&, double dt)
     {

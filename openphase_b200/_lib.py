@@ -96,6 +96,11 @@ _SIGS = {
     "opgpu_read_raw": (C.c_uint32, [_P, C.c_char_p]),
     "opgpu_write_raw": (C.c_uint32, [_P, C.c_char_p]),
     "opgpu_finalize_initialization": (C.c_uint32, [_P]),
+    "opgpu_write_grains": (C.c_uint32, [_P, C.c_char_p]),
+    "opgpu_read_grains": (C.c_uint32, [_P, C.c_char_p]),
+    "opgpu_write_vtk": (C.c_uint32, [_P, C.c_char_p]),
+    "opgpu_write_vtk_host": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32, _P, C.c_int32,
+                                          C.c_int32, C.c_int32, C.c_char_p]),
     "opgpu_total_entries": (C.c_uint32, [_P, C.POINTER(C.c_int64)]),
     "opgpu_download_lists": (C.c_uint32, [_P, _P, _P, _P]),
     "opgpu_download_flags": (C.c_uint32, [_P, _P]),

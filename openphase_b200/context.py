@@ -118,6 +118,29 @@ class Context:
     def write_raw(self, path):
         _check(lib().opgpu_write_raw(self.h, str(path).encode()), self.h, "write_raw")
 
+    def write_grains(self, path):
+        """Grain records in the reference's restart format (GrainsProperties::Write)."""
+        _check(lib().opgpu_write_grains(self.h, str(path).encode()), self.h, "write_grains")
+
+    def read_grains(self, path):
+        """Grain records from a restart file (GrainsProperties::Read); then finalize_initialization."""
+        _check(lib().opgpu_read_grains(self.h, str(path).encode()), self.h, "read_grains")
+
+    def write_restart(self, raw_path, grains_path):
+        """PhaseField::Write(Settings, tStep): the raw state and the grain records."""
+        self.write_raw(raw_path)
+        self.write_grains(grains_path)
+
+    def read_restart(self, raw_path, grains_path) -> int:
+        """PhaseField::Read(Settings, BC, tStep): raw state, grain records, then Finalize."""
+        self.read_raw(raw_path)
+        self.read_grains(grains_path)
+        return self.finalize_initialization()
+
+    def write_vtk(self, path):
+        """PhaseField::WriteVTK of the current state (.vts, ASCII)."""
+        _check(lib().opgpu_write_vtk(self.h, str(path).encode()), self.h, "write_vtk")
+
     def finalize_initialization(self) -> int:
         return _check(lib().opgpu_finalize_initialization(self.h), self.h, "finalize_initialization")
 
@@ -258,7 +281,9 @@ class Context:
 
     # ---- convenience
     @classmethod
-    def from_case(cls, case, precision="fp64", k_slots=8, device=0, state=None, threads=0):
+    def from_case(cls, case, precision="fp64", k_slots=8, device=0, state=None, threads=0, restart=None):
+        """A context holding the case's model, grains and parameters, and its initial state (or the
+        state of restart = (raw_path, grains_path) written by write_restart or by the reference)."""
         ctx = cls(case.nx, case.ny, case.nz, dx=case.dx, iwidth=case.iwidth, stencil=case.stencil,
                   gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
         ctx.set_model(case.sigma_phase(), case.mu_phase(), limit=case.limit_phase(), limiting=case.limiting,
@@ -273,6 +298,9 @@ class Context:
         if ps is not None:
             ctx.set_pair_table(ps, None)
         ctx.set_driving_force(case.driving_force())
+        if restart is not None:
+            ctx.read_restart(*restart)
+            return ctx
         counts, idx, val = state if state is not None else case.initial_state(threads)
         ctx.upload(counts, idx, val)
         ctx.finalize_initialization()

@@ -9,11 +9,12 @@
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cfloat>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -95,6 +96,7 @@ struct opgpu_ctx {
     double timed_ms = 0.0;
     double timed_classify_ms = 0.0;
     long long kernel_launches = 0;   // kernels of this library launched on the context's stream
+    int8_t* noalloc_scratch = nullptr;   // device address of the allocation-free flag scratch
 };
 
 namespace {
@@ -382,8 +384,9 @@ double disorientation_energy(const double* A, const double* B)
     return 0.349066 * constant * (0.8 - std::log(0.349066));
 }
 
-// Grain counts up to which the limited driving force is tabulated per grain pair (8 * G^2 bytes).
-constexpr int kMaxPairTableGrains = 16384;
+// Grain counts up to which the limited driving force is tabulated per grain pair (8 * G^2 bytes:
+// 3.2 GB of device memory at 20000 grains): every count the int16 grain indices allow.
+constexpr int kMaxPairTableGrains = 32767;
 
 // Stencil tables: LaplacianStencil3D_7 / _27a / _LB (include/Containers/LaplacianStencil.h:72-156)
 // and the neighbour sets of GradientStencil1D / 3D / 3D_LB (include/Containers/GradientStencil.h),
@@ -848,7 +851,7 @@ uint32_t refresh_pair_energy(opgpu_ctx* ctx)
     if (ctx->sp.pair_mode == OPGPU_PAIRS_HASH)
         return fail(ctx, OPGPU_E_INVALID, "DISORIENTATION energies are tabulated per grain pair: not with opgpu_set_pair_hash");
     if (G > kMaxPairTableGrains)
-        return fail(ctx, OPGPU_E_INVALID, "DISORIENTATION energies: at most 16384 grains");
+        return fail(ctx, OPGPU_E_INVALID, "DISORIENTATION energies: at most 32767 grains");
     const size_t GG = (size_t)G * G;
     std::vector<double> tab(GG);
     const double unit[4] = {1.0, 0.0, 0.0, 0.0};
@@ -1205,16 +1208,17 @@ extern "C" uint32_t opgpu_download_flags(opgpu_ctx* ctx, int8_t* flags)
 
 // ---- allocation-free flag download ------------------------------------------------------------
 // The flags are computed into a file-scope device array instead of a per-call cudaMalloc'd
-// buffer.  Its address is looked up once per device (cudaGetSymbolAddress, with that device
-// current) and cached.  Every one of the N bytes is written by flags_kernel before the copy, so
-// nothing in the scratch has to start at zero.  The scratch is shared by every context on a
-// device: overlapping calls race.
+// buffer.  Its address is looked up by each library context on its first call
+// (cudaGetSymbolAddress, with the context's device current) and kept in the context: a context
+// lives in one CUDA context (its own device buffers do), so the address cannot go stale even if the
+// host program resets a device and creates new contexts afterwards.  Every one of the N bytes is
+// written by flags_kernel before the copy, so nothing in the scratch has to start at zero.  The
+// scratch is shared by every context on a device: overlapping calls race.  The 16 MiB are reserved
+// when the library's device code is loaded on a device (at its first kernel use with lazy
+// loading), for every process that loads the library, whether or not this entry point is called.
 namespace {
 constexpr long long kNoAllocFlagsMax = 16LL << 20;   // bytes = voxels (a 256^3 grid)
-constexpr int kNoAllocMaxDevices = 64;
 __device__ __align__(256) int8_t g_noalloc_flags[kNoAllocFlagsMax];
-std::mutex g_noalloc_mu;
-int8_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 }  // namespace
 
 extern "C" uint32_t opgpu_download_flags_noalloc(opgpu_ctx* ctx, int8_t* flags)
@@ -1225,22 +1229,17 @@ extern "C" uint32_t opgpu_download_flags_noalloc(opgpu_ctx* ctx, int8_t* flags)
         return fail(ctx, OPGPU_E_INVALID,
                     "opgpu_download_flags_noalloc: grid of " + std::to_string(ctx->n) +
                     " voxels exceeds its fixed scratch of 16777216 voxels; use opgpu_download_flags");
-    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
-        return fail(ctx, OPGPU_E_INVALID, "opgpu_download_flags_noalloc: device ordinal above 63");
     if (!ctx->state_loaded) return fail(ctx, OPGPU_E_STATE, "no state");
-    int8_t* scratch = nullptr;
+    if (!ctx->noalloc_scratch)
     {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[ctx->device])
-        {
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_flags);
-            if (e != cudaSuccess)
-                return fail(ctx, OPGPU_E_CUDA, std::string("opgpu_download_flags_noalloc: set-up: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[ctx->device] = static_cast<int8_t*>(p);
-        }
-        scratch = g_noalloc_ptr[ctx->device];
+        // require() made the context's device current
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_flags);
+        if (e != cudaSuccess)
+            return fail(ctx, OPGPU_E_CUDA, std::string("opgpu_download_flags_noalloc: set-up: ") + cudaGetErrorString(e));
+        ctx->noalloc_scratch = static_cast<int8_t*>(p);
     }
+    int8_t* scratch = ctx->noalloc_scratch;
     const long long N = ctx->n;
     flags_kernel<<<grid_for(N, 256), 256, 0, ctx->stream>>>(ctx->grid.nx, ctx->grid.ny, ctx->grid.nz,
                                                              ctx->cnt[ctx->cur], scratch);
@@ -1743,4 +1742,306 @@ extern "C" uint32_t opgpu_step_complete(opgpu_ctx* ctx, const double* dev_src, i
     const uint32_t st = read_status(ctx);
     if (st & OPGPU_E_CUDA) return st;
     return st & OPGPU_SOFT_MASK;
+}
+
+// ---- restart files and visual output -----------------------------------------------------------
+
+namespace {
+
+// GrainStages of the reference (include/GrainsProperties.h:35-40): Seed 0, Nucleus 1, Stable 2.
+int stage_to_reference(int s) { return s == OPGPU_STAGE_SEED ? 0 : (s == OPGPU_STAGE_NUCLEUS ? 1 : 2); }
+int stage_from_reference(int s) { return s == 0 ? OPGPU_STAGE_SEED : (s == 1 ? OPGPU_STAGE_NUCLEUS : OPGPU_STAGE_STABLE); }
+
+template <class T>
+void put_bytes(std::vector<unsigned char>& b, T x)
+{
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&x);
+    b.insert(b.end(), p, p + sizeof(T));
+}
+
+template <class T>
+T get_bytes(const unsigned char*& p)
+{
+    T x;
+    std::memcpy(&x, p, sizeof(T));
+    p += sizeof(T);
+    return x;
+}
+
+// One grain record of GrainsProperties' binary file (Grain::Write, include/GrainsProperties.h:197-231):
+// Exist, Mobile (bool); Stage (int); Parent, Phase, Variant (size_t); State (int); Density, RefVolume,
+// Volume, MAXVolume; per axis Rcm, Vcm, Acm, aVel, aAcc, Force, Torque and a row of InertiaM; the
+// orientation quaternion (s, x, y, z).
+constexpr size_t kGrainRecordBytes = 2 * 1 + 4 + 3 * 8 + 4 + 4 * 8 + 3 * 10 * 8 + 4 * 8;
+
+}  // namespace
+
+extern "C" uint32_t opgpu_write_grains(opgpu_ctx* ctx, const char* path)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0 && path, "opgpu_write_grains: no grains or no path")) return r;
+    const int G = ctx->G;
+    std::vector<double> vol(G), maxv(G), refv(G);
+    std::vector<int32_t> ex(G), st(G);
+    if (uint32_t r = opgpu_grains(ctx, vol.data(), nullptr, maxv.data(), ex.data(), st.data())) return r;
+    CK(cudaMemcpy(refv.data(), ctx->d_refvol, G * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<unsigned char> b;
+    b.reserve(8 + (size_t)G * kGrainRecordBytes);
+    put_bytes<uint64_t>(b, (uint64_t)G);
+    for (int g = 0; g < G; g++)
+    {
+        const int ph = ctx->h_gphase.empty() ? 0 : ctx->h_gphase[g];
+        put_bytes<uint8_t>(b, ex[g] ? 1 : 0);             // Exist
+        put_bytes<uint8_t>(b, 1);                         // Mobile (reference default)
+        put_bytes<int32_t>(b, stage_to_reference(st[g]));
+        put_bytes<uint64_t>(b, 0);                        // Parent
+        put_bytes<uint64_t>(b, (uint64_t)ph);             // Phase
+        put_bytes<uint64_t>(b, 0);                        // Variant
+        put_bytes<int32_t>(b, ctx->sp.solid_p[ph] ? 0 : 1);   // State: AggregateStates Solid 0, Liquid 1
+        put_bytes<double>(b, 0.0);                        // Density (no equilibrium density here)
+        put_bytes<double>(b, refv[g]);
+        put_bytes<double>(b, vol[g]);
+        put_bytes<double>(b, maxv[g]);
+        for (int i = 0; i < 30; i++) put_bytes<double>(b, 0.0);   // rigid-body motion: not modelled
+        for (int i = 0; i < 4; i++)
+            put_bytes<double>(b, ctx->h_quat.empty() ? (i == 0 ? 1.0 : 0.0) : ctx->h_quat[4 * (size_t)g + i]);
+    }
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, OPGPU_E_IO, std::string("cannot open ") + path);
+    const bool ok = std::fwrite(b.data(), 1, b.size(), f) == b.size();
+    if (std::fclose(f) != 0 || !ok) return fail(ctx, OPGPU_E_IO, std::string("write failed: ") + path);
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_read_grains(opgpu_ctx* ctx, const char* path)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->G > 0 && path, "opgpu_read_grains: call opgpu_set_grains first")) return r;
+    if (ctx->initialized) return fail(ctx, OPGPU_E_STATE, "opgpu_read_grains: read the grains before the state is finalized");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, OPGPU_E_IO, std::string("cannot open ") + path);
+    std::vector<unsigned char> b;
+    unsigned char chunk[65536];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) b.insert(b.end(), chunk, chunk + got);
+    std::fclose(f);
+    const int G = ctx->G;
+    if (b.size() < 8) return fail(ctx, OPGPU_E_IO, "opgpu_read_grains: truncated file");
+    const unsigned char* p = b.data();
+    const uint64_t size = get_bytes<uint64_t>(p);
+    if (size != (uint64_t)G) return fail(ctx, OPGPU_E_INVALID, "opgpu_read_grains: the file holds a different number of grains");
+    if (b.size() != 8 + (size_t)G * kGrainRecordBytes) return fail(ctx, OPGPU_E_IO, "opgpu_read_grains: file size does not match its grain count");
+    std::vector<int16_t> ph(G);
+    std::vector<int8_t> ex(G), st(G);
+    std::vector<double> refv(G), vol(G), maxv(G), vr(G), quat(4 * (size_t)G);
+    bool rotated = false;
+    for (int g = 0; g < G; g++)
+    {
+        ex[g] = get_bytes<uint8_t>(p) ? 1 : 0;
+        (void)get_bytes<uint8_t>(p);                      // Mobile
+        st[g] = (int8_t)stage_from_reference(get_bytes<int32_t>(p));
+        (void)get_bytes<uint64_t>(p);                     // Parent
+        const uint64_t phase = get_bytes<uint64_t>(p);
+        if (phase >= (uint64_t)ctx->sp.nphases) return fail(ctx, OPGPU_E_INVALID, "opgpu_read_grains: phase out of range");
+        ph[g] = (int16_t)phase;
+        (void)get_bytes<uint64_t>(p);                     // Variant
+        (void)get_bytes<int32_t>(p);                      // State
+        (void)get_bytes<double>(p);                       // Density
+        refv[g] = get_bytes<double>(p);
+        vol[g] = get_bytes<double>(p);
+        maxv[g] = get_bytes<double>(p);
+        vr[g] = maxv[g] / refv[g];                        // Grain::Read (include/GrainsProperties.h:98)
+        p += 30 * sizeof(double);
+        for (int i = 0; i < 4; i++) quat[4 * (size_t)g + i] = get_bytes<double>(p);
+        rotated |= quat[4 * (size_t)g] != 1.0 || quat[4 * (size_t)g + 1] != 0.0 || quat[4 * (size_t)g + 2] != 0.0 ||
+                   quat[4 * (size_t)g + 3] != 0.0;
+    }
+    CK(cudaMemcpy(ctx->d_gphase, ph.data(), G * sizeof(int16_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_gstage, st.data(), G, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_exist, ex.data(), G, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_refvol, refv.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_volume, vol.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_maxvol, maxv.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_vr, vr.data(), G * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->h_gphase = ph;
+    ctx->dg_pair_dirty = true;
+    ctx->pair_energy_dirty = true;
+    return opgpu_set_orientations(ctx, rotated ? quat.data() : nullptr);
+}
+
+namespace {
+
+// Append the %.16g / integer text of one VTK point-data array in x-fastest order, formatted by
+// OpenMP threads over z-planes (the reference streams the same text, VTK::ForEach,
+// include/VTK.h:70-81).
+template <class F>
+void vtk_array(std::string& out, int nx, int ny, int nz, bool integral, F value)
+{
+    std::vector<std::string> part(nz);
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < nz; k++)
+    {
+        std::string& s = part[k];
+        s.reserve((size_t)nx * ny * 18);
+        char buf[40];
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++)
+            {
+                const long long v = ((long long)i * ny + j) * nz + k;
+                const double x = value(v);
+                const int len = integral ? std::snprintf(buf, sizeof(buf), "%lld\n", (long long)x)
+                                         : std::snprintf(buf, sizeof(buf), "%.16g\n", x);
+                s.append(buf, len);
+            }
+    }
+    for (auto& s : part) out += s;
+    out += "</DataArray>\n";
+}
+
+void vtk_header(std::string& out, const char* type, const std::string& name)
+{
+    out += std::string("<DataArray type = \"") + type + "\" Name = \"" + name +
+           "\" NumberOfComponents=\"1\" format=\"ascii\">\n";
+}
+
+}  // namespace
+
+extern "C" uint32_t opgpu_write_vtk_host(int32_t nx, int32_t ny, int32_t nz, const int32_t* counts, const int32_t* idx,
+                                         const double* val, int32_t ngrains, const int32_t* grain_phase,
+                                         int32_t nphases, int32_t laplacian_stencil, int32_t gradient_stencil,
+                                         const char* path)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !counts || !path || ngrains < 1 || nphases < 1 || nphases > kMaxPhases)
+        return OPGPU_E_INVALID;
+    if (laplacian_stencil < 0 || laplacian_stencil > 2 || gradient_stencil < 0 || gradient_stencil > 2)
+        return OPGPU_E_INVALID;
+    const long long N = (long long)nx * ny * nz;
+    std::vector<long long> off(N + 1, 0);
+    for (long long v = 0; v < N; v++) off[v + 1] = off[v] + counts[v];
+    for (long long e = 0; e < off[N]; e++)
+        if (idx[e] < 0 || idx[e] >= ngrains) return OPGPU_E_INVALID;
+    auto phase_of = [&](int g) { return grain_phase ? grain_phase[g] : 0; };
+    for (int g = 0; g < ngrains; g++)
+        if (phase_of(g) < 0 || phase_of(g) >= nphases) return OPGPU_E_INVALID;
+    StepParams sp{};
+    set_stencils(sp, laplacian_stencil, gradient_stencil, 1.0);
+    auto wrap = [](int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); };
+    // NodePF flag (PhaseField::SetFlagsSR, src/PhaseField.cpp:953-969) and the list length after
+    // CalculateDerivativesSR (src/PhaseField.cpp:566-615): stored fields plus the zero-valued
+    // candidates every stencil neighbour brings to a flag != 0 voxel
+    std::vector<int8_t> flag(N);
+    std::vector<int32_t> junctions(N);
+#pragma omp parallel for schedule(static)
+    for (long long v = 0; v < N; v++)
+    {
+        const int x = (int)(v / ((long long)ny * nz)), y = (int)((v / nz) % ny), z = (int)(v % nz);
+        int f = counts[v] > 1 ? 2 : 0;
+        for (int dx = -1; dx <= 1 && f == 0; dx++)
+            for (int dy = -1; dy <= 1 && f == 0; dy++)
+                for (int dz = -1; dz <= 1 && f == 0; dz++)
+                {
+                    const long long u = ((long long)wrap(x + dx, nx) * ny + wrap(y + dy, ny)) * nz + wrap(z + dz, nz);
+                    if (counts[u] > 1) f = 1;
+                }
+        flag[v] = (int8_t)f;
+        int n = counts[v];
+        if (f != 0)
+        {
+            std::vector<int32_t> seen(idx + off[v], idx + off[v + 1]);
+            for (int q = 0; q < sp.ns + sp.ng; q++)
+            {
+                const signed char* d = q < sp.ns ? sp.lap_d[q] : sp.grad_d[q - sp.ns];
+                const long long u = ((long long)wrap(x + d[0], nx) * ny + wrap(y + d[1], ny)) * nz + wrap(z + d[2], nz);
+                for (long long e = off[u]; e < off[u + 1]; e++)
+                    if (val[e] != 0.0 && std::find(seen.begin(), seen.end(), idx[e]) == seen.end()) seen.push_back(idx[e]);
+            }
+            n = (int)seen.size();
+        }
+        junctions[v] = n;
+    }
+    std::string out;
+    char line[160];
+    out += "<?xml version= \"1.0\" encoding=\"UTF-8\" standalone=\"yes\"?>\n";
+    out += "<VTKFile type=\"StructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n";
+    std::snprintf(line, sizeof(line), "<StructuredGrid WholeExtent=\"0 %d 0 %d 0 %d\">\n", nx - 1, ny - 1, nz - 1);
+    out += line;
+    out += "<PointData Scalars= \"ScalarData\">\n";
+    // PhaseField::Interfaces (src/PhaseField.cpp:3765-3777)
+    vtk_header(out, "Float64", "Interfaces");
+    vtk_array(out, nx, ny, nz, false, [&](long long v) {
+        double sum = 0.5;
+        if (flag[v] == 2)
+            for (long long a = off[v]; a < off[v + 1]; a++)
+                for (long long b = a + 1; b < off[v + 1]; b++) sum -= val[a] * val[b];
+        return 1.0 / (sum * 2.0);
+    });
+    vtk_header(out, "Int32", "Flags");
+    vtk_array(out, nx, ny, nz, true, [&](long long v) { return (double)flag[v]; });
+    // NodePF::majority_index (include/Containers/NodePF.h:194-211)
+    vtk_header(out, "Int32", "PhaseFields");
+    vtk_array(out, nx, ny, nz, true, [&](long long v) {
+        if (junctions[v] == 1) return (double)idx[off[v]];
+        double mv = 0.0;
+        int mi = 0;
+        for (long long a = off[v]; a < off[v + 1]; a++)
+            if (val[a] > mv) { mv = val[a]; mi = idx[a]; }
+        return (double)mi;
+    });
+    // PhaseField::CalculateFractions (src/PhaseField.cpp:411-423)
+    for (int ph = 0; ph < nphases; ph++)
+    {
+        vtk_header(out, "Float64", "PhaseFraction_" + std::to_string(ph));
+        vtk_array(out, nx, ny, nz, false, [&](long long v) {
+            double s = 0.0;
+            for (long long a = off[v]; a < off[v + 1]; a++)
+                if (phase_of(idx[a]) == ph) s += val[a];
+            return s;
+        });
+    }
+    vtk_header(out, "UInt64", "Junctions");
+    vtk_array(out, nx, ny, nz, true, [&](long long v) { return (double)junctions[v]; });
+    // Variant and Parent of the majority grain: 0 for every grain here (PhaseField::Variants,
+    // ::ParentGrain, src/PhaseField.cpp:3793-3839)
+    vtk_header(out, "Float64", "Variants");
+    vtk_array(out, nx, ny, nz, false, [&](long long) { return 0.0; });
+    vtk_header(out, "Float64", "ParentGrain");
+    vtk_array(out, nx, ny, nz, false, [&](long long) { return 0.0; });
+    out += "</PointData>\n";
+    // VTK::WriteCoordinates (include/VTK.h:420-471), single resolution
+    out += "<Points>\n";
+    out += "<DataArray type = \"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
+    {
+        std::vector<std::string> part(nz);
+#pragma omp parallel for schedule(dynamic)
+        for (int k = 0; k < nz; k++)
+        {
+            char buf[80];
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++)
+                    part[k].append(buf, std::snprintf(buf, sizeof(buf), "%d %d %d\n", i, j, k));
+        }
+        for (auto& s : part) out += s;
+    }
+    out += "</DataArray>\n";
+    out += "</Points>\n";
+    out += "</StructuredGrid>\n";
+    out += "</VTKFile>\n";
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return OPGPU_E_IO;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    return (std::fclose(f) == 0 && ok) ? OPGPU_OK : OPGPU_E_IO;
+}
+
+extern "C" uint32_t opgpu_write_vtk(opgpu_ctx* ctx, const char* path)
+{
+    if (uint32_t r = require(ctx, ctx && ctx->state_loaded && path, "opgpu_write_vtk: no state")) return r;
+    int64_t total = 0;
+    if (uint32_t r = opgpu_total_entries(ctx, &total)) return r;
+    std::vector<int32_t> counts(ctx->n), idx(total), gp(ctx->G);
+    std::vector<double> val(total);
+    if (uint32_t r = opgpu_download_lists(ctx, counts.data(), idx.data(), val.data())) return r;
+    for (int g = 0; g < ctx->G; g++) gp[g] = ctx->h_gphase.empty() ? 0 : ctx->h_gphase[g];
+    const uint32_t r = opgpu_write_vtk_host(ctx->grid.nx, ctx->grid.ny, ctx->grid.nz, counts.data(), idx.data(),
+                                            val.data(), ctx->G, gp.data(), ctx->sp.nphases,
+                                            ctx->grid.laplacian_stencil, ctx->grid.gradient_stencil, path);
+    if (r) return fail(ctx, r, std::string("opgpu_write_vtk: cannot write ") + path);
+    return OPGPU_OK;
 }

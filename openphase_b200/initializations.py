@@ -193,3 +193,21 @@ def quaternions(ngrains: int, seed: int) -> np.ndarray:
         z, w = b * np.sin(2 * np.pi * u3), b * np.cos(2 * np.pi * u3)
         q[g] = (w, x, y, z)
     return q
+
+
+def write_vtk(path, nx: int, ny: int, nz: int, counts, idx, val, grain_phase=None, nphases: int = 1,
+              stencil: str = "LB", gradient_stencil: str = "ISOTROPIC"):
+    """PhaseField::WriteVTK of ragged host lists (no device needed; opgpu_write_vtk_host)."""
+    from ._lib import STENCIL
+    c = np.ascontiguousarray(counts, dtype=np.int32)
+    i = np.ascontiguousarray(idx, dtype=np.int32)
+    v = np.ascontiguousarray(val, dtype=np.float64)
+    ngrains = int(i.max()) + 1 if i.size else 1
+    gp = None
+    if grain_phase is not None:
+        gp = np.ascontiguousarray(grain_phase, dtype=np.int32)
+        ngrains = gp.size
+    rc = lib().opgpu_write_vtk_host(nx, ny, nz, ptr(c), ptr(i), ptr(v), ngrains, ptr(gp), nphases,
+                                    STENCIL[stencil], STENCIL[gradient_stencil], str(path).encode())
+    if rc:
+        raise OpgpuError(rc, "write_vtk_host")

@@ -3,7 +3,8 @@
 Runs the reference (compiled from its own sources by `make -C oracle ref`, driven through its public
 API by oracle/ref_driver.cpp) on small seeded cases and stores, per case, the states and grain
 records at a few checkpoints.  The fixtures pin the oracle (tests/test_oracle.py) without needing the
-reference at test time.
+reference at test time.  OUTPUT_CASES also store the reference's VTK file and grain-record restart
+file of one state (tests/test_output_files.py).
 
     python tests/golden/make_golden.py [name ...]  # writes tests/golden/<name>.npz (all by default)
 """
@@ -94,7 +95,34 @@ GOLDEN_CASES = {
 }
 
 
+# output files of the reference (PhaseField::WriteVTK and the grain-record restart file) for a state
+# of each case at one step: they pin opgpu_write_vtk_host and the grain-record format
+OUTPUT_CASES = {
+    "vtk_pairs_12": (Case(12, 10, 8, 8, seed=5, iwidth=3.0, dt=0.1, sigma=1.2, sigma_pairs=(0.8, 0.4),
+                          dg_scale=0.05, name="vtk_pairs_12"), 5),
+    "vtk_simple_nuclei_12": (Case(12, 12, 10, 4, seed=6, iwidth=3.0, dt=0.05, sigma=1.2, stencil="SIMPLE",
+                                  phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                                  phase_solid=(0, 1), phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=3.0,
+                                  name="vtk_simple_nuclei_12"), 4),
+}
+
+
+def output_fixture(name):
+    case, step = OUTPUT_CASES[name]
+    counts, idx, val = case.initial_state()
+    res, stats = run_reference(case, counts, idx, val, [step], threads=2, vtk_steps=(step,))
+    c, i, v, vol, vr = res[step]
+    arrays = {"counts": c.astype(np.uint8), "idx": i.astype(np.int16), "val": v, "volume": vol,
+              "volume_ratio": vr, "vtk": np.frombuffer(stats["vtk"][step], dtype=np.uint8),
+              "grains_file": np.frombuffer(stats["grains_file"][step], dtype=np.uint8)}
+    np.savez_compressed(HERE / f"{name}.npz", **arrays)
+    print(name, arrays["vtk"].size, arrays["grains_file"].size)
+
+
 def main(names=None):
+    for name in OUTPUT_CASES:
+        if not names or name in names:
+            output_fixture(name)
     for name, (case, steps) in GOLDEN_CASES.items():
         if names and name not in names:
             continue

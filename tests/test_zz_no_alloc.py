@@ -28,6 +28,23 @@ def test_flags_noalloc_matches_flags(precision):
         ctx.step(case.dt, 3)
 
 
+def test_flags_noalloc_allocates_no_device_memory():
+    """The property the entry point exists for: after its one-time set-up, calls leave the device's
+    free memory unchanged (no allocation, not even a transient one that a free would hide from a
+    before/after count in the caller's memory pool)."""
+    import torch
+    case = Case(40, 36, 32, 12, seed=22, iwidth=5.0, dt=0.1, name="noalloc_mem")
+    ctx = Context.from_case(case, precision="fp64", k_slots=16)
+    ref = ctx.flags()
+    ctx.flags_noalloc()                       # one-time set-up of this context
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert np.array_equal(ctx.flags_noalloc(), ref)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_flags_noalloc_rejects_grid_beyond_scratch():
     ctx = Context(257, 256, 256, iwidth=5.0, precision="fp32", k_slots=8)
     with pytest.raises(OpgpuError) as e:
