@@ -2,8 +2,9 @@
 
     python -m openphase_b200.build_ext            # builds openphase_b200/lib/libopgpu.so
 
-Every .cu translation unit is compiled by nvcc for sm_100a only; step_f64.cu additionally with
---fmad=false (the FP64 form reproduces the reference's unfused double arithmetic).  The host-side
+Every .cu translation unit is compiled by nvcc for sm_100a only; step_f64.cu, step_f32.cu and
+adjoint.cu additionally with --fmad=false (the FP64 form reproduces the reference's unfused double
+arithmetic; the adjoint repeats the forward's per-voxel arithmetic of either form exactly).  The host-side
 initialisers are compiled by the system g++ with OpenMP.  Objects go to openphase_b200/_build/.
 """
 from __future__ import annotations
@@ -28,7 +29,7 @@ NVCC_COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp",
 CU_UNITS = {
     "opgpu.cu": [],
     "step_f64.cu": ["--fmad=false"],
-    "step_f32.cu": ["--fmad=true"],
+    "step_f32.cu": ["--fmad=false"],
     "adjoint.cu": ["--fmad=false"],
 }
 CPP_UNITS = ["host_init.cpp"]

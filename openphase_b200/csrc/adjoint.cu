@@ -513,7 +513,10 @@ __device__ void limiter_iteration_reverse(int n, const double* val, double dt, c
 // The adjoint of one wide voxel's step, from its list (own fields first, then candidates) with the
 // values and Laplacians the step used.  KL: capacity of the working arrays (the list-length
 // kernels pass their exact length, so that every loop has a fixed trip count).
-template <int KL, int KS>
+// R: the precision of the forward step's per-voxel arithmetic (the state's); the pair kinetics are
+// recomputed in it, operation by operation as the forward kernels do (every unit compiled without
+// contraction), so that the recomputed increments and every decision after them are the forward's.
+template <int KL, int KS, class R = double>
 __device__ __forceinline__ void adjoint_core(const StepParams& p, const StepArrays& a, const AdjArrays& aa,
                                              long long v, int flag, int n, int c, const int16_t* g0,
                                              const double* val_in, const double* lap_in, uint32_t st)
@@ -547,37 +550,46 @@ __device__ __forceinline__ void adjoint_core(const StepParams& p, const StepArra
     const double norm_1 = 1.0 / localN;
     const double pref = p.pref_do;
     double psi[KP], pv0[KP], pv[KP], lpv[KP], lpw[KP];
-    for (int i = 0; i < n; i++)
     {
-        const double vri = a.vr[g[i]];
-        for (int j = i + 1; j < n; j++)
+        // the forward's arithmetic in R (list_compute_kernel / warp_general_kernel / list_step)
+        const R norm_1r = (R)(1.0 / localN);
+        const R prefr = (R)p.pref_do;
+        for (int i = 0; i < n; i++)
         {
-            const int q = pair_pos(i, j, n);
-            const double vrj = a.vr[g[j]];
-            const double scale = (vri == 1.0 && vrj == 1.0) ? 1.0 : sqrt(vri * vrj);
-            const double h = 0.5 * (1.0 + scale) * pref;
-            double dphi = pair_energy(p, a, g[i], g[j]) * ((lap[i] + h * val[i]) - (lap[j] + h * val[j]));
-            if (n > 2)
+            const double vri = a.vr[g[i]];
+            const R vi = (R)val[i], li = (R)lap[i];
+            for (int j = i + 1; j < n; j++)
             {
-                for (int k = 0; k < n; k++)
+                const int q = pair_pos(i, j, n);
+                const double vrj = a.vr[g[j]];
+                const R scale = (vri == 1.0 && vrj == 1.0) ? R(1) : (R)sqrt(vri * vrj);
+                const R h = R(0.5) * (R(1) + scale) * prefr;
+                const R vj = (R)val[j];
+                R dphi = (R)pair_energy(p, a, g[i], g[j]) * ((li + h * vi) - ((R)lap[j] + h * vj));
+                if (n > 2)
                 {
-                    if (k == i || k == j) continue;
-                    const double sbk = pair_energy(p, a, g[j], g[k]);
-                    const double sak = pair_energy(p, a, g[i], g[k]);
-                    dphi += (sbk - sak) * (lap[k] + h * val[k]);
-                    if (p.tj_factor != 0.0 || scale < 1.0)
+                    for (int k = 0; k < n; k++)
                     {
-                        const int pA = a.gphase[g[i]], pB = a.gphase[g[j]], pG = a.gphase[g[k]];
-                        const int P = p.nphases;
-                        const double tj = dmax_ref(p.tj_factor, 1.0 - scale);
-                        dphi += tj * pref * ((p.sigma_p[pA * P + pB] + p.sigma_p[pB * P + pG]) + p.sigma_p[pA * P + pG])
-                              * (val[i] * val[k] - val[j] * val[k]);
+                        if (k == i || k == j) continue;
+                        const R sbk = (R)pair_energy(p, a, g[j], g[k]);
+                        const R sak = (R)pair_energy(p, a, g[i], g[k]);
+                        const R vk = (R)val[k];
+                        dphi += (sbk - sak) * ((R)lap[k] + h * vk);
+                        if (p.tj_factor != 0.0 || scale < R(1))
+                        {
+                            const int pA = a.gphase[g[i]], pB = a.gphase[g[j]], pG = a.gphase[g[k]];
+                            const int P = p.nphases;
+                            const R tj = (R)dmax_ref(p.tj_factor, (double)(R(1) - scale));
+                            dphi += tj * prefr
+                                  * (((R)p.sigma_p[pA * P + pB] + (R)p.sigma_p[pB * P + pG]) + (R)p.sigma_p[pA * P + pG])
+                                  * (vi * vk - vj * vk);
+                        }
                     }
                 }
+                psi[q] = (double)dphi;
+                dphi *= (R)pair_mobility(p, a, g[i], g[j]) * norm_1r * scale;
+                pv0[q] = (double)dphi;
             }
-            psi[q] = dphi;
-            dphi *= pair_mobility(p, a, g[i], g[j]) * norm_1 * scale;
-            pv0[q] = dphi;
         }
     }
     const bool with_dg = p.use_dg && flag == 2;
@@ -589,7 +601,7 @@ __device__ __forceinline__ void adjoint_core(const StepParams& p, const StepArra
                 const double locdG = limited_force(p, a, g[i], g[j]);
                 double norm = sqrt(val[i] * val[j]);
                 if (a.gstage[g[i]] == 1 || a.gstage[g[j]] == 1) norm += 1.0e-6;
-                pv0[pair_pos(i, j, n)] += locdG * pair_mobility(p, a, g[i], g[j]) * norm * p.pref_df;
+                pv0[pair_pos(i, j, n)] += locdG * (double)(R)pair_mobility(p, a, g[i], g[j]) * norm * p.pref_df;
             }
     }
     // ---- forward recompute: projection ----
@@ -893,7 +905,7 @@ __global__ void __launch_bounds__(128) adjoint_list_kernel(const __grid_constant
             own = own && val[k] != 0.0;
             c += own ? 1 : 0;
         }
-        adjoint_core<N, KS>(p, a, aa, v, flag, N, c, g, val, lap, 0u);
+        adjoint_core<N, KS, R>(p, a, aa, v, flag, N, c, g, val, lap, 0u);
     }
 }
 
@@ -917,7 +929,7 @@ __global__ void __launch_bounds__(64) adjoint_worklist_kernel(const __grid_const
                                          nullptr, st);
         double val[KL], lap[KL];
         for (int k = 0; k < n; k++) { val[k] = (double)vr[k]; lap[k] = (double)lr[k]; }
-        adjoint_core<KL, KS>(p, a, aa, v, flag, n, c, g, val, lap, st);
+        adjoint_core<KL, KS, R>(p, a, aa, v, flag, n, c, g, val, lap, st);
     }
 }
 

@@ -1,5 +1,7 @@
 // FP32 form of the fused step: field values, increments and stencil arithmetic in FP32; the
-// simplex sums (limiter sums, finalize total) and the grain-volume reduction stay in FP64.
+// simplex sums (limiter sums, finalize total) and the grain-volume reduction stay in FP64.  This
+// translation unit is compiled with --fmad=false: the adjoint recomputes the per-voxel FP32
+// arithmetic operation by operation and must round exactly as the forward did.
 #include "tile_kernel.cuh"
 
 namespace opgpu {

@@ -87,6 +87,14 @@ struct TileSmem {
 
 __device__ __forceinline__ unsigned slot_hash(int g) { return ((unsigned)g * 2654435761u) >> 26; }
 
+// One term of the classify kernel's dense-plane Laplacian.  FP64: the reference's separate multiply
+// and add (the FP64 unit is compiled without contraction).  FP32: one fused multiply-add, written
+// out because the FP32 unit is compiled without contraction too (so that the adjoint can repeat its
+// per-voxel arithmetic exactly); these Laplacians reach the forward and the adjoint alike through
+// the work records, so their rounding only has to be the same in both, which it is.
+__device__ __forceinline__ double lap_acc(double l, double w, double x) { return l + w * x; }
+__device__ __forceinline__ float lap_acc(float l, float w, float x) { return __fmaf_rn(w, x, l); }
+
 // Slot of a grain in the window (-1 if the grain has none).
 __device__ __forceinline__ int find_slot(const int* hkey, const uint8_t* hslot, int g)
 {
@@ -494,7 +502,7 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
                 const int dx = stencil_dx<NS>(q);
                 const int pl = dx < 0 ? sl0 : (dx > 0 ? sl2 : sl1);
                 const int r = rec0 + stencil_dy<NS>(q) * kC + stencil_dz<NS>(q);
-                l += (R)p.lap_w[q] * S.dense[s][pl][r];
+                l = lap_acc(l, (R)p.lap_w[q], S.dense[s][pl][r]);
             }
             rg[k] = (int16_t)S.grain_of[s];
             rv[k] = S.dense[s][sl1][rec0];

@@ -152,6 +152,9 @@ def test_fp32_and_fp64_gradients_agree():
         ctx, R, *_ = _setup(precision=prec)
         R.forward()
         grads[prec] = R.backward(w)
+        # the reverse sweep recomputes every step in the forward's own precision and order: the
+        # recomputed lists are the stored ones (no adjoint mismatch) in both forms
+        assert R.adjoint_status == 0, (prec, R.adjoint_status)
     for a, b in zip(grads["fp64"], grads["fp32"]):
         assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(a)
 
