@@ -874,10 +874,11 @@ template <class R, int N, int KS>
 __global__ void __launch_bounds__(128) adjoint_list_kernel(const __grid_constant__ StepParams p, const StepArrays a,
                                                             const AdjArrays aa, int nslices)
 {
-    // the entries of length N from all classify slices form one index range, split evenly
+    // the entries of length N from all classify slices form one index range, split evenly in whole
+    // multiples of the block size (every thread of a block that has work gets some)
     const unsigned* __restrict__ off = a.bucket_off + (long long)N * (nslices + 1);
     const unsigned total = off[nslices];
-    const unsigned per = ((total + gridDim.x * 32u - 1u) / (gridDim.x * 32u)) * 32u;
+    const unsigned per = ((total + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x)) * blockDim.x;
     const unsigned r0 = blockIdx.x * per;
     if (r0 >= total) return;
     const unsigned r1 = min(total, r0 + per);

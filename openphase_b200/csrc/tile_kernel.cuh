@@ -575,7 +575,10 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
     const int t = threadIdx.x;
     const unsigned* __restrict__ off = a.bucket_off + (long long)N * (nslices + 1);
     const unsigned total = off[nslices];
-    const unsigned per = ((total + gridDim.x * 32u - 1u) / (gridDim.x * 32u)) * 32u;
+    // whole chunks of 32 entries for every warp of the block: a length with few entries then keeps
+    // all warps of fewer blocks busy instead of one warp of many blocks (the others would wait at
+    // the final barrier, holding their registers)
+    const unsigned per = ((total + gridDim.x * blockDim.x - 1u) / (gridDim.x * blockDim.x)) * blockDim.x;
     const unsigned r0 = blockIdx.x * per;
     if (r0 >= total) return;
     const unsigned r1 = min(total, r0 + per);
