@@ -218,6 +218,59 @@ def slab_run(case, precision, k_slots, steps, warmup, device, state, sigma, dg, 
     return out
 
 
+def scale_run(steps, warmup, device, k_slots=16, threads=0):
+    """The 512^3 scale set-up (134M voxels, 20000 Voronoi grains, eta = 6, sigma ~ U[0.8, 1.2] per
+    grain pair generated on the device, dG ~ U[0, 0.05], dt = 0.08): device-resident step time of
+    both forms over steps warmup+1 .. warmup+steps.  The checkpointed adjoint is not run at this
+    size: sqrt(1000)-interval checkpointing keeps about 65 states of 13 GB (K = 16, FP32)."""
+    import torch
+    from openphase_b200.cases import scale_512
+    from openphase_b200.context import Context
+
+    case = scale_512()
+    t = time.time()
+    state = case.initial_state(threads)
+    t_init = time.time() - t
+    dg = case.driving_force()
+    lo, span = case.sigma_pairs
+    out = {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains, "k_slots": k_slots,
+           "pair_energies": "generated on the device (opgpu_set_pair_hash)", "initial_state_seconds": round(t_init, 1),
+           "adjoint": "not run: sqrt(1000)-interval checkpointing needs about 65 states of 13 GB (K = 16, FP32)"}
+    for precision in ("fp64", "fp32"):
+        s = 4 if precision == "fp32" else 8
+        ctx = Context(case.nx, case.ny, case.nz, dx=case.dx, iwidth=case.iwidth, stencil=case.stencil,
+                      gradient_stencil=case.gradient_stencil, precision=precision, k_slots=k_slots, device=device)
+        ctx.set_model([[case.sigma]], [[case.mu]], limit=[[case.limit]], limiting=case.limiting,
+                      regularization=case.regularization)
+        ctx.set_grains(case.ngrains)
+        ctx.set_pair_hash(case.seed, lo, span)
+        ctx.set_driving_force(dg)
+        ctx.upload(*state)
+        ctx.finalize_initialization()
+        ctx.step(case.dt, warmup)
+        stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0 = ctx.stats()
+        torch.cuda.synchronize(device)
+        with ClockSampler(device) as clk:
+            e0.record(stream)
+            ctx.step_async(case.dt, steps)
+            e1.record(stream)
+            torch.cuda.synchronize(device)
+        status = ctx.sync()
+        ms = e0.elapsed_time(e1)
+        s1 = ctx.stats()
+        wide = (s1["wide_total"] - s0["wide_total"]) / steps
+        ctx.close()
+        out[precision] = {"value": case.n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+                          "state_bytes_per_buffer": case.n * (1 + k_slots * (2 + s)),
+                          "wide_fraction": wide / case.n, "status": int(status), "clocks": clk.summary(),
+                          "roofline_frac": (wide * 2 * (1 + 8 * (2 + s)) + case.n) / (ms / steps / 1e3) / 1e9
+                                           / measured_peaks()[0]}
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def e2e_run(case, precision, k_slots, steps, device, state, sigma, dg):
     """End to end through the C ABI with pinned host buffers; host<->device copies inside the clock."""
     import torch
@@ -357,6 +410,15 @@ def cpu_baseline(case, state, threads, warmup, steps=3):
     return d
 
 
+def build_record():
+    """Which library ran: its build stamp, and whether that is the hash of the sources in this tree."""
+    from openphase_b200 import build_ext
+    from openphase_b200._lib import lib
+    info = lib().opgpu_build_info().decode()
+    tree = build_ext.source_hash()
+    return {"library": info, "tree_source_hash": tree, "built_from_this_tree": info.endswith(tree)}
+
+
 def workload_config(case, k_slots, world):
     """The `config` object of both arms' lines."""
     return {"workload": case.name, "grid": [case.nx, case.ny, case.nz], "grains": case.ngrains,
@@ -399,6 +461,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-fp32-error", action="store_true")
+    ap.add_argument("--no-scale", action="store_true")
     ap.add_argument("--workload", default="grain_growth_dg_256")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -501,6 +564,10 @@ def main():
     if not args.no_adjoint and world == 1:
         adjoint = adjoint_run(local_rank)
 
+    scale = None
+    if not args.no_scale and world == 1 and args.workload == "grain_growth_dg_256":
+        scale = scale_run(args.steps, args.warmup, local_rank, threads=threads)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, state, os.cpu_count() or 1, args.warmup)
@@ -527,9 +594,11 @@ def main():
                  "gpu_launches": f32["gpu_launches"], "error": fp32_error},
         "fp32_over_fp64": f32["value"] / f64["value"],
         "adjoint": adjoint,
+        "scale_512": scale,
         "status": {"fp32": f32["status"], "fp64": f64["status"]},
         "wide_fraction": f64["wide_fraction"],
         "initial_state_seconds": round(t_init, 2),
+        "build": build_record(),
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -134,6 +134,9 @@ uint32_t opgpu_create(const opgpu_grid* grid, opgpu_ctx** out);
 uint32_t opgpu_destroy(opgpu_ctx* ctx);
 const char* opgpu_last_error(const opgpu_ctx* ctx);
 int32_t  opgpu_abi_version(void);
+/* Build stamp: "opgpu sm_100a source <hash>", the hash of the sources and compile flags the library
+ * was built from (openphase_b200/build_ext.py: source_hash).  No reference counterpart. */
+const char* opgpu_build_info(void);
 /* Number of CUDA devices visible (0 without a GPU). */
 int32_t  opgpu_device_count(void);
 

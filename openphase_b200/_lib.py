@@ -84,6 +84,7 @@ _SIGS = {
     "opgpu_destroy": (C.c_uint32, [_P]),
     "opgpu_last_error": (C.c_char_p, [_P]),
     "opgpu_abi_version": (C.c_int32, []),
+    "opgpu_build_info": (C.c_char_p, []),
     "opgpu_step_save_input": (C.c_uint32, [_P, C.c_double, C.c_int32]),
     "opgpu_device_count": (C.c_int32, []),
     "opgpu_set_model": (C.c_uint32, [_P, C.POINTER(Model)]),

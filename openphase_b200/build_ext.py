@@ -65,11 +65,31 @@ def _run(cmd, verbose):
     subprocess.run(cmd, check=True, env=_env())
 
 
+def source_hash() -> str:
+    """SHA-256 (first 16 hex digits) over the library's sources, headers and compile flags: the
+    build stamp the library reports through opgpu_build_info()."""
+    import hashlib
+    h = hashlib.sha256()
+    files = sorted([*CSRC.glob("*.cu"), *CSRC.glob("*.cpp"), *CSRC.glob("*.h"), *CSRC.glob("*.cuh"),
+                    *INCLUDE.glob("*.h")], key=lambda f: f.name)
+    for f in files:
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    h.update(repr((ARCH, [x for x in NVCC_COMMON if not x.startswith("/")], CU_UNITS)).encode())
+    return h.hexdigest()[:16]
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     LIBDIR.mkdir(exist_ok=True)
     nvcc = _nvcc()
     hdrs = _headers()
+    stamp = source_hash()
+    # the stamp is compiled into opgpu.cu; rebuild it when the stamp changes
+    stamp_file = BUILD / "source_hash.txt"
+    if not stamp_file.exists() or stamp_file.read_text() != stamp:
+        stamp_file.write_text(stamp)
+        hdrs = hdrs + [stamp_file]
     objs = []
     jobs = []
     for unit, extra in CU_UNITS.items():
@@ -77,7 +97,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         obj = BUILD / (unit + ".o")
         objs.append(obj)
         if force or _stale(obj, [src, *hdrs]):
-            jobs.append([nvcc, *ARCH, *NVCC_COMMON, *extra, "-c", str(src), "-o", str(obj)])
+            jobs.append([nvcc, *ARCH, *NVCC_COMMON, *extra, f"-DOPGPU_SOURCE_HASH=\"{stamp}\"", "-c", str(src),
+                         "-o", str(obj)])
     for unit in CPP_UNITS:
         src = CSRC / unit
         obj = BUILD / (unit + ".o")

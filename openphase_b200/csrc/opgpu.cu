@@ -494,6 +494,14 @@ uint32_t require(opgpu_ctx* ctx, bool cond, const char* what)
 
 extern "C" int32_t opgpu_abi_version(void) { return OPGPU_ABI_VERSION; }
 
+#ifndef OPGPU_SOURCE_HASH
+#define OPGPU_SOURCE_HASH "unstamped"
+#endif
+extern "C" const char* opgpu_build_info(void)
+{
+    return "opgpu sm_100a source " OPGPU_SOURCE_HASH;
+}
+
 extern "C" int32_t opgpu_device_count(void)
 {
     int n = 0;
