@@ -35,6 +35,8 @@ extern "C" {
 #define OPGPU_E_LIMITER_CAP     (1u << 4)  /* increment limiter stopped after its 25 iterations       */
 #define OPGPU_E_NONFINITE       (1u << 5)  /* a non-finite phase-field value was produced             */
 #define OPGPU_E_ADJOINT_MISMATCH (1u << 6) /* adjoint step: recomputed step differs from the stored one */
+#define OPGPU_E_AVERAGE_SKIPPED (1u << 7)  /* driving-force averaging could not store a voxel's pairs;
+                                              that voxel's pairs kept the raw force                      */
 /* hard errors */
 #define OPGPU_E_INVALID         (1u << 8)  /* invalid argument                                         */
 #define OPGPU_E_CUDA            (1u << 9)  /* CUDA runtime error (message: opgpu_last_error)           */
@@ -159,6 +161,16 @@ uint32_t opgpu_set_pair_hash(opgpu_ctx* ctx, uint64_t seed, double lo, double sp
  * src/DrivingForce.cpp:176-183, NodeDF.h:412-435, then Average->SkipAverage :242-274).
  * NULL disables the driving-force merge. */
 uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG);
+/* Driving-force averaging, $Average Yes of @DrivingForce (the reference default; the benchmark
+ * set-ups use No): DrivingForce::Average -> SetWeights, CollectAverage, DistributeAverage
+ * (src/DrivingForce.cpp:242-256, 276-478) in the default PHASEFIELDS weights mode, run on the state
+ * each step starts from.  range ($Range) <= 0: iWidth; threshold ($Threshold) <= 0: iWidth/15 below
+ * an interface width of 5 cells, else 1/3.  The averaged force of a pair replaces its raw force in
+ * the merge (a pair whose weight exceeds the threshold nowhere within range gets none, as in the
+ * reference).  Costs two passes over a sphere of radius range per interface pair, 8 bytes of device
+ * memory per voxel and 16 per pair of stored fields of the interface voxels, and one host
+ * synchronisation per step; not with the adjoint, the tangent-linear model or slab steps. */
+uint32_t opgpu_set_averaging(opgpu_ctx* ctx, int32_t enable, int32_t range, double threshold);
 /* Grain orientations as quaternions (s, x, y, z) per grain, quat[4*G] (GrainsProperties::Orientation,
  * include/GrainsProperties.h:76); NULL = unrotated.  Used by anisotropic energy models. */
 uint32_t opgpu_set_orientations(opgpu_ctx* ctx, const double* quat);

@@ -20,6 +20,7 @@ E_NORMALIZE_WARN = 1 << 3
 E_LIMITER_CAP = 1 << 4
 E_NONFINITE = 1 << 5
 E_ADJOINT_MISMATCH = 1 << 6
+E_AVERAGE_SKIPPED = 1 << 7
 E_INVALID = 1 << 8
 E_CUDA = 1 << 9
 E_IO = 1 << 10
@@ -35,6 +36,7 @@ _CODE_NAMES = {
     E_OVERFLOW_K: "OVERFLOW_K", E_OVERFLOW_LIST: "OVERFLOW_LIST", E_EMPTY_VOXEL: "EMPTY_VOXEL",
     E_NORMALIZE_WARN: "NORMALIZE_WARN", E_LIMITER_CAP: "LIMITER_CAP", E_NONFINITE: "NONFINITE",
     E_ADJOINT_MISMATCH: "ADJOINT_MISMATCH",
+    E_AVERAGE_SKIPPED: "AVERAGE_SKIPPED",
     E_INVALID: "INVALID", E_CUDA: "CUDA", E_IO: "IO", E_STATE: "STATE", E_NODEVICE: "NODEVICE",
 }
 
@@ -93,6 +95,7 @@ _SIGS = {
     "opgpu_set_pair_hash": (C.c_uint32, [_P, C.c_uint64, C.c_double, C.c_double]),
     "opgpu_set_driving_force": (C.c_uint32, [_P, _P]),
     "opgpu_set_orientations": (C.c_uint32, [_P, _P]),
+    "opgpu_set_averaging": (C.c_uint32, [_P, C.c_int32, C.c_int32, C.c_double]),
     "opgpu_upload_lists": (C.c_uint32, [_P, _P, _P, _P]),
     "opgpu_read_raw": (C.c_uint32, [_P, C.c_char_p]),
     "opgpu_write_raw": (C.c_uint32, [_P, C.c_char_p]),

@@ -31,6 +31,7 @@ CU_UNITS = {
     "step_f64.cu": ["--fmad=false"],
     "step_f32.cu": ["--fmad=false"],
     "adjoint.cu": ["--fmad=false"],
+    "average.cu": ["--fmad=false"],
 }
 CPP_UNITS = ["host_init.cpp"]
 

@@ -40,6 +40,7 @@ class Case:
     sigma_pairs: Optional[tuple] = None   # (lo, span): per-grain-pair sigma table
     dg_scale: float = 0.0             # per-grain driving force scale (0 = none)
     limiting: bool = True
+    average: bool = False             # DrivingForce $Average (reference default Yes; the benchmarks use No)
     limit: float = 0.95
     regularization: float = 1.0
     tj_factor: float = 0.0

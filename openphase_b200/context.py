@@ -83,6 +83,10 @@ class Context:
                   mobility_model=as_ptr(mm, C.c_int32), mobility_eps=as_ptr(mme, C.c_double))
         _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
 
+    def set_averaging(self, enable: bool, range_: int = 0, threshold: float = 0.0):
+        """DrivingForce $Average Yes/No (with $Range, $Threshold; 0 = the reference defaults)."""
+        _check(lib().opgpu_set_averaging(self.h, int(enable), int(range_), float(threshold)), self.h, "set_averaging")
+
     def set_orientations(self, quat):
         q = None if quat is None else np.ascontiguousarray(quat, dtype=np.float64)
         _check(lib().opgpu_set_orientations(self.h, ptr(q)), self.h, "set_orientations")
@@ -298,6 +302,8 @@ class Context:
         if ps is not None:
             ctx.set_pair_table(ps, None)
         ctx.set_driving_force(case.driving_force())
+        if getattr(case, "average", False):
+            ctx.set_averaging(True)
         if restart is not None:
             ctx.read_restart(*restart)
             return ctx

@@ -97,6 +97,18 @@ struct opgpu_ctx {
     double timed_classify_ms = 0.0;
     long long kernel_launches = 0;   // kernels of this library launched on the context's stream
     int8_t* noalloc_scratch = nullptr;   // device address of the allocation-free flag scratch
+    // driving-force averaging ($Average Yes)
+    bool averaging = false;
+    int avg_range = 0;
+    double avg_threshold = 0.0;
+    double *d_df_tmp = nullptr, *d_df_lim = nullptr;
+    unsigned *d_df_npairs = nullptr, *d_df_off = nullptr;
+    unsigned long long* d_df_total = nullptr;
+    unsigned df_cap = 0;
+    void* d_df_scan = nullptr;
+    size_t df_scan_bytes = 0;
+    signed char* d_avg_off = nullptr;
+    int avg_noff = 0;
 };
 
 namespace {
@@ -594,6 +606,8 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     dfree(ctx->d_wl);
     dfree(ctx->d_bucket); dfree(ctx->d_bucket_count); dfree(ctx->d_bucket_off);
     dfree(ctx->d_facets);
+    dfree(ctx->d_df_tmp); dfree(ctx->d_df_lim); dfree(ctx->d_avg_off);
+    dfree(ctx->d_df_npairs); dfree(ctx->d_df_off); dfree(ctx->d_df_scan); dfree(ctx->d_df_total);
     dfree(ctx->d_status);
     dfree(ctx->d_counters);
     for (auto& s : ctx->slots)
@@ -807,6 +821,52 @@ extern "C" uint32_t opgpu_set_driving_force(opgpu_ctx* ctx, const double* dG)
         ctx->dg_pair_dirty = true;
     }
     ctx->sp.use_dg = 1;
+    return OPGPU_OK;
+}
+
+extern "C" uint32_t opgpu_set_averaging(opgpu_ctx* ctx, int32_t enable, int32_t range, double threshold)
+{
+    if (uint32_t r = require(ctx, ctx != nullptr, "opgpu_set_averaging: no context")) return r;
+    if (!enable)
+    {
+        ctx->averaging = false;
+        return OPGPU_OK;
+    }
+    // DrivingForce::Initialize / ReadInput (src/DrivingForce.cpp:61-73, 132-133): Range = iWidth,
+    // Threshold = iWidth/15 below an interface width of 5 cells, else 1/3
+    const double iw = ctx->grid.iwidth;
+    const int R = range > 0 ? range : (int)iw;
+    const double t = threshold > 0.0 ? threshold : (iw < 5.0 ? iw / 15.0 : 1.0 / 3.0);
+    if (R < 1 || !(t < 1.0)) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_averaging: range >= 1 and threshold < 1 required");
+    // the sphere of CollectAverage / DistributeAverage in their loop order: offsets with
+    // Range - |d| > 0 within +-min(Range, N - 1) per axis
+    const int Xr = std::min(R, ctx->grid.nx - 1), Yr = std::min(R, ctx->grid.ny - 1), Zr = std::min(R, ctx->grid.nz - 1);
+    std::vector<signed char> off;
+    for (int ii = -Xr; ii <= Xr; ii++)
+        for (int jj = -Yr; jj <= Yr; jj++)
+            for (int kk = -Zr; kk <= Zr; kk++)
+            {
+                const double wd = R - std::sqrt((double)(ii * ii + jj * jj + kk * kk));
+                if (wd > 0.0) off.insert(off.end(), {(signed char)ii, (signed char)jj, (signed char)kk});
+            }
+    if (R > 127) return fail(ctx, OPGPU_E_INVALID, "opgpu_set_averaging: range above 127");
+    dfree(ctx->d_avg_off);
+    ctx->d_avg_off = nullptr;
+    CK(dalloc(&ctx->d_avg_off, off.size()));
+    CK(cudaMemcpy(ctx->d_avg_off, off.data(), off.size(), cudaMemcpyHostToDevice));
+    if (!ctx->d_df_npairs)
+    {
+        // pair slots are sized per step (they grow to the total the scan finds)
+        CK(dalloc(&ctx->d_df_total, 1));
+        CK(dalloc(&ctx->d_df_npairs, (size_t)ctx->n));
+        CK(dalloc(&ctx->d_df_off, (size_t)ctx->n));
+        ctx->df_scan_bytes = average_scan_bytes(ctx->n);
+        CK(dalloc(reinterpret_cast<unsigned char**>(&ctx->d_df_scan), ctx->df_scan_bytes));
+    }
+    ctx->avg_noff = (int)(off.size() / 3);
+    ctx->avg_range = R;
+    ctx->avg_threshold = t;
+    ctx->averaging = true;
     return OPGPU_OK;
 }
 
@@ -1076,6 +1136,40 @@ static uint32_t enqueue_steps(opgpu_ctx* ctx, double dt, int nsteps, bool partia
         a.dg_pair = pair_table ? ctx->d_dg_pair : nullptr;
         a.grot = ctx->d_grot; a.facets = ctx->d_facets;
         a.vol_acc = ctx->d_vol_acc; a.status = ctx->d_status; a.counters = ctx->d_counters;
+        a.df_lim = nullptr;
+        if (ctx->averaging && sp.use_dg)
+        {
+            // DrivingForce::Average on the state the step starts from: slots for every pair of stored
+            // fields of the interface voxels (grown to the total this state needs), then the passes
+            AvgArrays aa{ctx->d_df_npairs, ctx->d_df_off, ctx->d_df_tmp, ctx->d_df_lim, ctx->df_cap,
+                         ctx->d_avg_off, ctx->avg_noff, std::sqrt(ctx->avg_threshold * (1.0 - ctx->avg_threshold)),
+                         ctx->d_df_scan, ctx->df_scan_bytes};
+            int rc = launch_average_scan(ctx->n, aa, ctx->cnt[in], ctx->d_df_total, ctx->stream);
+            if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("averaging scan: ") + cudaGetErrorString((cudaError_t)rc));
+            unsigned long long total = 0;
+            CK(cudaMemcpyAsync(&total, ctx->d_df_total, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (total > 0xFFFFFFF0ULL) return fail(ctx, OPGPU_E_INVALID, "averaging: more than 2^32 pair slots");
+            if (total > ctx->df_cap)
+            {
+                dfree(ctx->d_df_tmp); dfree(ctx->d_df_lim);
+                ctx->d_df_tmp = ctx->d_df_lim = nullptr;
+                const unsigned long long cap = std::min<unsigned long long>(total + total / 4 + 1024, 0xFFFFFFF0ULL);
+                CK(dalloc(&ctx->d_df_tmp, (size_t)cap));
+                CK(dalloc(&ctx->d_df_lim, (size_t)cap));
+                ctx->df_cap = (unsigned)cap;
+                aa.tmp = ctx->d_df_tmp;
+                aa.lim = ctx->d_df_lim;
+                aa.cap = ctx->df_cap;
+            }
+            rc = launch_average(sp, aa, ctx->cnt[in], ctx->idx[in], ctx->val[in], ctx->fp32 != 0,
+                                ctx->d_vr, ctx->d_dg, ctx->d_gphase, ctx->d_status, ctx->stream);
+            if (rc != 0) return fail(ctx, OPGPU_E_CUDA, std::string("averaging: ") + cudaGetErrorString((cudaError_t)rc));
+            ctx->kernel_launches += 5;   // count, scan, total, collect, distribute
+            a.df_lim = ctx->d_df_lim;
+            a.df_off = ctx->d_df_off;
+            a.df_cap = ctx->df_cap;
+        }
         a.slow_list = ctx->d_slow_list; a.slow_count = ctx->d_slow_count; a.slow_cap = (unsigned)ctx->n;
         a.wl = ctx->d_wl; a.wl_slice = ctx->wl_slice;
         a.bucket = ctx->d_bucket; a.bucket_count = ctx->d_bucket_count; a.bucket_off = ctx->d_bucket_off;
@@ -1400,6 +1494,8 @@ uint32_t refresh_dg_pair(opgpu_ctx* ctx)
 
 uint32_t ensure_adjoint(opgpu_ctx* ctx)
 {
+    if (ctx->averaging)
+        return fail(ctx, OPGPU_E_INVALID, "the adjoint and tangent-linear steps do not support driving-force averaging");
     if (ctx->adjoint_ready) return OPGPU_OK;
     const size_t N = (size_t)ctx->n, K = (size_t)ctx->K, G = (size_t)ctx->G;
     for (int b = 0; b < 2; b++) CK(dalloc(&ctx->d_lam[b], N * K));
@@ -1416,6 +1512,8 @@ uint32_t ensure_adjoint(opgpu_ctx* ctx)
 
 uint32_t ensure_tlm(opgpu_ctx* ctx)
 {
+    if (ctx->averaging)
+        return fail(ctx, OPGPU_E_INVALID, "the adjoint and tangent-linear steps do not support driving-force averaging");
     if (ctx->tlm_ready) return OPGPU_OK;
     const size_t N = (size_t)ctx->n, K = (size_t)ctx->K, G = (size_t)ctx->G;
     for (int b = 0; b < 2; b++) CK(dalloc(&ctx->d_dphi[b], N * K));
@@ -1720,6 +1818,8 @@ extern "C" uint32_t opgpu_volume_recount(opgpu_ctx* ctx)
 
 extern "C" uint32_t opgpu_step_partial(opgpu_ctx* ctx, double dt)
 {
+    if (ctx && ctx->averaging)
+        return fail(ctx, OPGPU_E_INVALID, "opgpu_step_partial: a slab holds one halo plane; averaging needs Range planes");
     if (uint32_t r = enqueue_steps(ctx, dt, 1, true)) return r;
     return opgpu_sync(ctx);
 }

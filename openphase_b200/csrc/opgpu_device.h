@@ -24,6 +24,24 @@ enum : uint32_t {
     kStLimiterCap = 1u << 4,
     kStNonFinite = 1u << 5,
     kStAdjointMismatch = 1u << 6,   // the recomputed step does not reproduce the stored next state
+    kStAverageSkipped = 1u << 7,    // driving-force averaging ran out of its pair storage for a voxel
+                                    // (its pairs kept the raw force)
+};
+
+// Driving-force averaging (average.cu).  Every interface voxel's pairs of stored fields get one
+// slot each in compact storage: off[v] is the voxel's first slot (exclusive scan of c(c-1)/2 over
+// the voxels with c > 1 stored fields); a voxel whose slots would pass cap is skipped.
+struct AvgArrays {
+    unsigned* npairs;            // [N] pairs of stored fields of interface voxels, then scanned into off
+    unsigned* off;               // [N] first slot of each voxel
+    double* tmp;                 // [cap] CollectAverage's tmp per stored pair
+    double* lim;                 // [cap] the averaged, limited force per stored pair
+    unsigned cap;
+    const signed char* off3;     // [noff][3] sphere offsets with Range - |d| > 0, in loop order
+    int noff;
+    double weight_threshold;     // sqrt(Threshold (1 - Threshold))
+    void* scan_tmp;              // device scratch of the scan
+    size_t scan_bytes;
 };
 
 // counters[] slots: the step kernel adds into the per-step slots 0-2; the grain-update kernel rolls
@@ -110,6 +128,9 @@ struct StepArrays {
     const double* pair_sigma;  // [G*G] or null
     const double* pair_mu;     // [G*G] or null
     const double* dg_pair;     // [G*G] limited driving force per grain pair, or null (evaluated in place)
+    const double* df_lim;      // averaged limited force per stored pair (slot df_off[v] + pair), or null
+    const unsigned* df_off;    // [N] first pair slot of each voxel (averaging)
+    unsigned df_cap;           // pair slots
     const double* grot;        // [G*9] grain rotation matrices (row-major), for anisotropic energies
     double* vol_acc;           // [G] volume accumulator of the output state (zeroed by the caller)
     uint32_t* status;          // soft status bits
@@ -168,6 +189,14 @@ int launch_step_f32(const StepParams& p, const StepArrays& a, int k_slots, int v
 // The classify kernel of the tiled step alone; returns the number of classify blocks or < 0.
 int launch_classify_f64(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
 int launch_classify_f32(const StepParams& p, const StepArrays& a, int k_slots, void* stream);
+// Driving-force averaging of a state (average.cu): launch_average_scan counts the pair slots of
+// every voxel, scans them into aa.off and writes their total to d_total; launch_average then writes
+// aa.tmp and aa.lim.  average_scan_bytes gives the scan's scratch bytes for n voxels.
+size_t average_scan_bytes(long long n);
+int launch_average_scan(long long n, const AvgArrays& aa, const uint8_t* cnt, unsigned long long* d_total, void* stream);
+int launch_average(const StepParams& p, const AvgArrays& aa, const uint8_t* cnt, const int16_t* idx,
+                   const void* val, bool fp32, const double* vr, const double* dg, const int16_t* gphase,
+                   uint32_t* status, void* stream);
 // Add the volumes of the window planes of a state to vol_acc (defined in step_f64.cu).
 int launch_volume_recount(const StepParams& p, const uint8_t* cnt, const int16_t* idx, const void* val, int fp32,
                           double* vol_acc, void* stream);

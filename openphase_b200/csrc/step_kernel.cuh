@@ -66,6 +66,21 @@ __device__ __forceinline__ double limited_force(const StepParams& p, const StepA
     return locdG;
 }
 
+// The limited driving force of list entries i < j of an interface voxel v with c stored fields (the
+// leading entries of its list): with driving-force averaging, the averaged force of a pair of
+// stored fields; else, and for the zero-valued candidates (weight 0: their force is multiplied by
+// 0 unless a Seed takes part, which the reference gives the raw force), the pair's own force.
+__device__ __forceinline__ double pair_force(const StepParams& p, const StepArrays& a, long long v, int c, int i,
+                                             int j, int gi, int gj)
+{
+    if (a.df_lim && j < c)
+    {
+        const unsigned o = a.df_off[v];
+        if ((unsigned long long)o + (unsigned)(c * (c - 1) / 2) <= a.df_cap) return a.df_lim[o + pair_pos(i, j, c)];
+    }
+    return limited_force(p, a, gi, gj);
+}
+
 // Slice of entry e of one list length in the concatenated length buckets: the s with
 // off[s] <= e < off[s + 1] (off[nslices] > e).
 __device__ __forceinline__ int slice_of(const unsigned* __restrict__ off, int nslices, unsigned e)
@@ -293,11 +308,11 @@ __device__ __forceinline__ double voxel_energy(const StepParams& p, const StepAr
 }
 
 // Stages 2-5 for a list of n fields (own fields first, then candidates, as CalculateDerivativesSR
-// leaves them) with their Laplacians.  Leaves the new record (the fields that survive finalize, in
-// list order) in sc.g / sc.val and returns its length.
+// leaves them) with their Laplacians, of voxel v with c stored fields.  Leaves the new record (the
+// fields that survive finalize, in list order) in sc.g / sc.val and returns its length.
 template <class R>
 __device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& a, const ListScratch<R>& sc, int n,
-                                         int flag, uint32_t& st)
+                                         int flag, uint32_t& st, long long v, int c)
 {
     const int S = sc.stride;
 #define G_(k) sc.g[(k) * S]
@@ -371,7 +386,7 @@ __device__ __forceinline__ int list_step(const StepParams& p, const StepArrays& 
             for (int j = i + 1; j < n; j++)
             {
                 const int gj = G_(j);
-                const double locdG = limited_force(p, a, gi, gj);
+                const double locdG = pair_force(p, a, v, c, i, j, gi, gj);
                 double norm = sqrt(vi * (double)V_(j));
                 if (a.gstage[gi] == 1 || a.gstage[gj] == 1) norm += 1.0e-6;
                 const double mob = p.aniso ? voxel_mobility<R>(p, a, sc, i, j) : pair_mobility(p, a, gi, gj);
@@ -716,7 +731,7 @@ __device__ __forceinline__ void voxel_step_generic(const StepParams& p, const St
     R grad[ANISO ? 3 * KL : 1];
     const int n = gather_list<R, KL>(p, cnt, gin, vin, nb, v, gL, val, lap, ANISO ? grad : nullptr, st);
     const ListScratch<R> sc{gL, val, lap, sg, pv, pos, neg, 1, ANISO ? grad : nullptr};
-    int m = list_step<R>(p, a, sc, n, flag, st);
+    int m = list_step<R>(p, a, sc, n, flag, st, v, (int)cnt[v]);
     if (m > KS) { st |= kStOverflowK; m = KS; }
     a.cnt_out[v] = (uint8_t)m;
     for (int i = 0; i < m; i++)

@@ -34,7 +34,7 @@ class OpParams(C.Structure):
                 ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
                 ("limiting", C.c_int), ("limit_phase", C.c_void_p), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int),
-                ("nucleus_volume_factor", C.c_double), ("threads", C.c_int)]
+                ("nucleus_volume_factor", C.c_double), ("threads", C.c_int), ("average", C.c_int)]
 
 
 _olib = None
@@ -133,7 +133,8 @@ class Oracle:
                      quat=_p(quat).value if quat is not None else None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
                      dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
                      limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
-                     consider_nucleus_volume=1, nucleus_volume_factor=1.0, threads=threads)
+                     consider_nucleus_volume=1, nucleus_volume_factor=1.0, threads=threads,
+                     average=int(getattr(case, "average", False)))
         self.case = case
         self.h = L.op_create(C.byref(p), cap)
         if not self.h:
@@ -222,7 +223,7 @@ def _case_text(case, workdir: Path, dump_steps, threads, nsteps=None, vtk_steps=
     nsteps = max(dump_steps) if nsteps is None else nsteps
     lines = [f"nx {case.nx}", f"ny {case.ny}", f"nz {case.nz}", f"dx {case.dx!r}", f"iwidth {case.iwidth!r}",
              f"stencil {case.stencil}", f"dt {case.dt!r}", f"nsteps {nsteps}", f"nphases {P}",
-             f"ngrains {case.ngrains}", f"limiting {int(case.limiting)}",
+             f"ngrains {case.ngrains}", f"limiting {int(case.limiting)}", f"average {int(case.average)}",
              f"regularization {case.regularization!r}", f"tj_factor {case.tj_factor!r}",
              "dump_steps " + " ".join(str(s) for s in dump_steps)]
     if vtk_steps:

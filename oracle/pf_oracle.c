@@ -53,6 +53,11 @@ struct op_sim {
     int ns; int sdi[27], sdj[27], sdk[27]; double sw[27];
     int ng; int gdi[27], gdj[27], gdk[27]; double gw[27][3];
     uint32_t status;
+    /* driving-force averaging: per interface voxel, per pair of its positive entries (a < b in
+     * list order) the intermediate (tmp) and averaged driving force; npos[v] positive entries */
+    double *df_tmp, *df_avg;
+    int32_t* npos;
+    int maxpp;
 };
 
 static double dmax(double a, double b) { return (a < b) ? b : a; }   /* std::max */
@@ -286,6 +291,7 @@ op_sim* op_create(const op_params* p, int cap)
     s->max_volume = (double*)calloc(G, sizeof(double));
     s->ref_volume = (double*)calloc(G, sizeof(double));
     s->vr = (double*)calloc(G, sizeof(double));
+    s->npos = (int32_t*)calloc((size_t)s->n, sizeof(int32_t));
     s->exist = (int32_t*)calloc(G, sizeof(int32_t));
     s->stage = (int32_t*)calloc(G, sizeof(int32_t));
     /* PhaseField::AddGrainInfo (src/PhaseField.cpp:2970-2979) on a fresh Grain
@@ -314,6 +320,7 @@ void op_destroy(op_sim* s)
     free(s->mobility_model); free(s->mobility_eps);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
+    free(s->npos); free(s->df_tmp); free(s->df_avg);
     free(s->exist); free(s->stage);
     free(s);
 }
@@ -657,10 +664,139 @@ static int do_increments(const op_sim* s, const entry* L, int n, pair* P)
     return np;
 }
 
-/* DrivingForce::MergePhaseFieldIncrementsSR (src/DrivingForce.cpp:497-602) after SkipAverage
- * (:258-274) with $Average No, for the per-grain driving force raw(a,b) = dG_b - dG_a that the
- * oracle driver adds with NodeDF::add_raw for each pair (a before b) of an interface voxel. */
-static void df_merge(const op_sim* s, const entry* L, int n, pair* P)
+/* Driving-force averaging, DrivingForce::Average with $Average Yes (src/DrivingForce.cpp:242-256):
+ * SetWeights (:276-291), CollectAverage (:293-383) and DistributeAverage (:384-478) in the default
+ * PHASEFIELDS weights mode (:59, :137), with Range = iWidth and Threshold = iWidth/15 below an
+ * interface width of 5 cells, else 1/3 (:64-73), for the per-grain driving force raw(A,B) =
+ * dG_B - dG_A that the oracle driver adds on every pair of an interface voxel.  Only the pairs of
+ * positive entries have a weight; the entries of the zero-valued candidates keep weight 0, tmp 0
+ * and average 0 (raw for a Seed). */
+static int df_range(const op_sim* s) { return (int)s->p.iwidth; }   /* int Range = double iWidth */
+
+static double df_threshold(const op_sim* s)
+{
+    return s->p.iwidth < 5.0 ? s->p.iwidth/15.0 : 1.0/3.0;
+}
+
+/* Force(u).get_weight(A, B): sqrt(phi_A*phi_B) of an interface voxel u holding both (SetWeights),
+ * 0 elsewhere; *sa, *sb get the list positions of A and B. */
+static double df_weight(const op_sim* s, long u, int A, int B, int* sa, int* sb)
+{
+    *sa = -1; *sb = -1;
+    if (s->flag[u] != 2) return 0.0;
+    const entry* L = s->e + u*s->cap;
+    for (int k = 0; k < s->cnt[u]; k++)
+    {
+        if (L[k].idx == A) *sa = k;
+        if (L[k].idx == B) *sb = k;
+    }
+    if (*sa < 0 || *sb < 0) return 0.0;
+    return sqrt(L[*sa].val*L[*sb].val);
+}
+
+static void df_average(op_sim* s)
+{
+    const int nx = s->p.nx, ny = s->p.ny, nz = s->p.nz;
+    const int R = df_range(s);
+    const int Xr = R < nx - 1 ? R : nx - 1, Yr = R < ny - 1 ? R : ny - 1, Zr = R < nz - 1 ? R : nz - 1;
+    const double thr = df_threshold(s);
+    const double weight_threshold = sqrt(thr*(1.0 - thr));
+    int maxpos = 2;
+    for (long v = 0; v < s->n; v++)
+    {
+        const entry* L = s->e + v*s->cap;
+        int c = 0;
+        while (c < s->cnt[v] && L[c].val > 0.0) c++;
+        s->npos[v] = c;
+        if (s->flag[v] == 2 && c > maxpos) maxpos = c;
+    }
+    const int maxpp = maxpos*(maxpos - 1)/2;
+    if (maxpp > s->maxpp)
+    {
+        free(s->df_tmp); free(s->df_avg);
+        s->df_tmp = (double*)malloc((size_t)s->n*maxpp*sizeof(double));
+        s->df_avg = (double*)malloc((size_t)s->n*maxpp*sizeof(double));
+        s->maxpp = maxpp;
+    }
+    const int MP = s->maxpp;
+    /* CollectAverage */
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (long v = 0; v < s->n; v++)
+    {
+        if (s->flag[v] != 2) continue;
+        const int i = (int)(v/((long)ny*nz)), j = (int)((v/nz) % ny), k = (int)(v % nz);
+        const entry* L = s->e + v*s->cap;
+        const int c = s->npos[v];
+        for (int a = 0; a < c; a++)
+        for (int b = a + 1; b < c; b++)
+        {
+            const int A = L[a].idx, B = L[b].idx;
+            const double raw = s->dg[B] - s->dg[A];
+            const double weight = sqrt(L[a].val*L[b].val);
+            const double scale = s->vr[A]*s->vr[B];
+            double tmp = 0.0;
+            if (weight > weight_threshold*scale)
+            {
+                double value = 0.0, sum_weights = 0.0;
+                for (int ii = -Xr; ii <= Xr; ii++)
+                for (int jj = -Yr; jj <= Yr; jj++)
+                for (int kk = -Zr; kk <= Zr; kk++)
+                {
+                    const double weight_dist = R - sqrt((double)(ii*ii + jj*jj + kk*kk));
+                    int sa, sb;
+                    const double weight_phi = df_weight(s, vox(s, i + ii, j + jj, k + kk), A, B, &sa, &sb);
+                    if (weight_dist > 0.0 && weight_phi > 0.0)
+                    {
+                        sum_weights += weight_phi;
+                        value += weight_phi*raw;   /* get_raw(A, B) at the neighbour: raw of (A, B) */
+                    }
+                }
+                tmp = sum_weights > 0.0 ? value/sum_weights : raw;
+            }
+            s->df_tmp[v*MP + pair_pos(a, b, c)] = tmp;
+        }
+    }
+    /* DistributeAverage */
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (long v = 0; v < s->n; v++)
+    {
+        if (s->flag[v] != 2) continue;
+        const int i = (int)(v/((long)ny*nz)), j = (int)((v/nz) % ny), k = (int)(v % nz);
+        const entry* L = s->e + v*s->cap;
+        const int c = s->npos[v];
+        for (int a = 0; a < c; a++)
+        for (int b = a + 1; b < c; b++)
+        {
+            const int A = L[a].idx, B = L[b].idx;
+            const double scale = s->vr[A]*s->vr[B];
+            double value = 0.0, sum_weights = 0.0;
+            for (int ii = -Xr; ii <= Xr; ii++)
+            for (int jj = -Yr; jj <= Yr; jj++)
+            for (int kk = -Zr; kk <= Zr; kk++)
+            {
+                const double weight_dist = R - sqrt((double)(ii*ii + jj*jj + kk*kk));
+                const long u = vox(s, i + ii, j + jj, k + kk);
+                int sa, sb;
+                const double weight_phi = df_weight(s, u, A, B, &sa, &sb);
+                if (weight_dist > 0.0 && weight_phi > weight_threshold*scale)
+                {
+                    sum_weights += weight_phi;
+                    /* get_tmp(A, B): the neighbour's tmp, negated when it lists B before A */
+                    const double t = s->df_tmp[u*MP + (sa < sb ? pair_pos(sa, sb, s->npos[u]) : pair_pos(sb, sa, s->npos[u]))];
+                    value += weight_phi*(sa < sb ? t : -t);
+                }
+            }
+            s->df_avg[v*MP + pair_pos(a, b, c)] =
+                sum_weights > 0.0 ? value/sum_weights : s->df_tmp[v*MP + pair_pos(a, b, c)];
+        }
+    }
+}
+
+/* DrivingForce::MergePhaseFieldIncrementsSR (src/DrivingForce.cpp:497-602) for the per-grain
+ * driving force raw(a,b) = dG_b - dG_a that the oracle driver adds with NodeDF::add_raw for each
+ * pair (a before b) of an interface voxel: locdG = raw (SkipAverage, $Average No, :258-274) or the
+ * average above ($Average Yes). */
+static void df_merge(const op_sim* s, long v, const entry* L, int n, pair* P)
 {
     const double Eta = s->p.iwidth*s->p.dx;
     const double Prefactor = OP_PI/Eta;
@@ -669,9 +805,16 @@ static void df_merge(const op_sim* s, const entry* L, int n, pair* P)
     for (int b = a + 1; b < n; b++)
     {
         const int ga = L[a].idx, gb = L[b].idx;
+        const int seed = s->stage[ga] == OP_STAGE_SEED || s->stage[gb] == OP_STAGE_SEED;
         double locdG = s->dg[gb] - s->dg[ga];
+        if (s->p.average)
+        {
+            const int c = s->npos[v];
+            if (b < c) locdG = s->df_avg[v*s->maxpp + pair_pos(a, b, c)];
+            else if (!seed) locdG = 0.0;   /* weight 0, no Seed: the average stays 0 (:464-468) */
+        }
         double norm = sqrt(L[a].val*L[b].val);
-        if (s->stage[ga] == OP_STAGE_SEED || s->stage[gb] == OP_STAGE_SEED) norm += 1.0e-6;
+        if (seed) norm += 1.0e-6;
         if (s->p.limiting)
         {
             const int pA = s->grain_phase[ga], pB = s->grain_phase[gb];
@@ -1020,6 +1163,7 @@ uint32_t op_step(op_sim* s, double dt, int nsteps)
     for (int t = 0; t < nsteps; t++)
     {
         uint32_t st = 0;
+        if (s->dg && s->p.average) df_average(s);
         #pragma omp parallel reduction(|:st)
         {
             pair* P = (pair*)malloc(maxpairs*sizeof(pair));
@@ -1030,7 +1174,7 @@ uint32_t op_step(op_sim* s, double dt, int nsteps)
                 entry* L = s->e + v*cap;
                 const int n = s->cnt[v];
                 const int np = do_increments(s, L, n, P);
-                if (s->dg && s->flag[v] == 2) df_merge(s, L, n, P);
+                if (s->dg && s->flag[v] == 2) df_merge(s, v, L, n, P);
                 st |= normalize(L, n, P, np, dt);
                 merge(L, P, np, dt);
             }

@@ -61,6 +61,8 @@ typedef struct op_params {
     int consider_nucleus_volume;      /* PhaseField ConsiderNucleusVolume (default 1)           */
     double nucleus_volume_factor;     /* PhaseField NucleusVolumeFactor (default 1)             */
     int threads;                      /* OpenMP threads (0 = runtime default)                   */
+    int average;                      /* DrivingForce $Average (reference default Yes; the
+                                         benchmark set-ups use No)                               */
 } op_params;
 
 typedef struct op_sim op_sim;

@@ -9,7 +9,8 @@
 //     IP.Set(Phi, BC)                             src/InterfaceProperties.cpp:557-576
 //     <per-grain-pair sigma/mu written into IP.Properties on wide-interface voxels>
 //     <per-grain driving force written with NodeDF::add_raw on interface voxels>
-//     dG.Average(Phi, BC)                         src/DrivingForce.cpp:242-256 (SkipAverage, $Average No)
+//     dG.Average(Phi, BC)                         src/DrivingForce.cpp:242-256 ($Average No: SkipAverage;
+//                                                 "average 1": SetWeights, CollectAverage, DistributeAverage)
 //     DO.CalculatePhaseFieldIncrements(Phi,IP,dG) src/DoubleObstacle.cpp:479-500
 //     dG.MergePhaseFieldIncrements(Phi, IP)       src/DrivingForce.cpp:480-602
 //     Phi.NormalizeIncrements(BC, dt)             src/PhaseField.cpp:1334-1349
@@ -71,6 +72,7 @@ struct Case
     std::vector<int> grain_phase;
     std::vector<double> pair_sigma, pair_mu, dg;
     bool limiting = true;
+    bool average = false;          // DrivingForce $Average
     double regularization = 1.0;
     double tj_factor = 0.0;
     bool consider_nucleus_volume = true;
@@ -141,6 +143,7 @@ static Case parse_case(const std::string& path)
         else if (key == "dg_file") is >> dg_file;
         else if (key == "orientation_file") is >> orientation_file;
         else if (key == "limiting") { int v; is >> v; c.limiting = v != 0; }
+        else if (key == "average") { int v; is >> v; c.average = v != 0; }
         else if (key == "regularization") is >> c.regularization;
         else if (key == "tj_factor") is >> c.tj_factor;
         else if (key == "consider_nucleus_volume") { int v; is >> v; c.consider_nucleus_volume = v != 0; }
@@ -225,7 +228,7 @@ static void write_opi(const Case& c, const std::string& path)
     o << "$TripleJunctionFactor : " << c.tj_factor << "\n";
     o << "$RegularizationFactor : " << c.regularization << "\n";
     o << "\n@DrivingForce\n";
-    o << "$Average : No\n";
+    o << "$Average : " << (c.average ? "Yes" : "No") << "\n";
     o << "$Limiting : " << (c.limiting ? "Yes" : "No") << "\n";
     for (int a = 0; a < c.nphases; a++)
     for (int b = a; b < c.nphases; b++)

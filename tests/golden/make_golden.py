@@ -92,6 +92,12 @@ GOLDEN_CASES = {
     "disorientation_20": (Case(20, 20, 20, 12, seed=11, iwidth=4.0, dt=0.1, orientations=True,
                                orientation_spread=0.6, disorientation=True, name="disorientation_20"),
                           [1, 40]),
+    # driving-force averaging ($Average Yes, the reference default): Range = iWidth, threshold
+    # iWidth/15 below 5 cells (first case) and 1/3 from 5 cells on (second case)
+    "average_20": (Case(20, 18, 16, 12, seed=21, iwidth=4.0, dt=0.1, sigma=1.2, sigma_pairs=(0.8, 0.4),
+                        dg_scale=0.1, average=True, name="average_20"), [1, 10, 20]),
+    "average_eta6_24": (Case(24, 24, 20, 10, seed=23, iwidth=6.0, dt=0.08, sigma=1.2, sigma_pairs=(0.8, 0.4),
+                             dg_scale=0.2, average=True, name="average_eta6_24"), [1, 10]),
 }
 
 
