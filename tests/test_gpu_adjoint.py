@@ -58,11 +58,11 @@ def test_tangent_state_equals_forward_and_dot_product():
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
 
 
-def _fd_check(h_rel, seed):
+def _fd_check(h_rel, seed, case=CASE, nsteps=T, interval=None, precision="fp64"):
     """Central differences on 32 random parameters (12 sigma pairs, 12 mu pairs, 8 driving forces)
     of L = sum_g w_g V_g(T); L is summed on the host in a fixed order (deterministic)."""
-    ctx, R, state, sig, mu, dg = _setup()
-    G = CASE.ngrains
+    ctx, R, state, sig, mu, dg = _setup(precision=precision, interval=interval, case=case, nsteps=nsteps)
+    G = case.ngrains
     rng = np.random.default_rng(seed)
     w = rng.standard_normal(G)
     R.forward()
@@ -178,3 +178,60 @@ def test_autograd_function_calibration_loss():
     assert np.allclose(s.grad.numpy(), gs, rtol=0, atol=1e-12 * np.abs(gs).max())
     assert np.allclose(m.grad.numpy(), gm, rtol=0, atol=1e-12 * np.abs(gm).max())
     assert np.allclose(d.grad.numpy(), gd, rtol=0, atol=1e-12 * max(np.abs(gd).max(), 1e-30))
+
+
+def test_calibration_rollout_gradients():
+    """The calibration set-up itself: 128^3, 256 Voronoi grains, sigma ~ U[0.8, 1.2] per pair,
+    dG ~ U[0, 0.03].
+
+    (1) 200 steps of the FP32 form, checkpoints every 16 steps, central differences at 1e-4
+        relative on 32 random parameters: a pair of perturbed rollouts that takes different
+        decisions (a field appears or vanishes somewhere in the 2M voxels, a limiter switches
+        branch) measures a jump, not the derivative.  At this size every pair does, so the count is
+        reported and the few kept pairs (if any) must agree within 1e-3.
+    (2) The derivative itself: the FP64 form over the first 30 steps, central differences at 1e-8
+        relative keep every decision; the median relative difference is <= 1e-3 and every
+        parameter agrees within 1e-3 of the largest gradient of its kind (small gradients are
+        swamped by the rounding of the loss, ~1e-16 |L| / h).
+    (3) The full 200-step checkpointed rollout in FP64: the tangent-linear model and the adjoint
+        satisfy the dot-product identity to 1e-10."""
+    import json
+    from openphase_b200.cases import adjoint_calibration_128
+    case = adjoint_calibration_128()
+    G = case.ngrains
+    picks, smooth, jumps = _fd_check(1e-4, 5, case=case, nsteps=case.nsteps, interval=16, precision="fp32")
+    rels = sorted(r[4] for r in smooth + jumps)
+    print("FD_CALIBRATION_FP32_1e-4 " + json.dumps({"steps": case.nsteps, "parameters": len(picks),
+                                                    "decisions_kept": len(smooth), "decisions_changed": len(jumps),
+                                                    "median_rel": rels[len(rels) // 2]}))
+    for kind, ix, fd, ad, rel in smooth:
+        assert rel <= 1e-3, (kind, ix, fd, ad, rel)
+    # (2)
+    picks, smooth, jumps = _fd_check(1e-8, 5, case=case, nsteps=30, precision="fp64")
+    rels = sorted(r[4] for r in smooth)
+    scale = {k: max(abs(r[3]) for r in smooth if r[0] == k) for k in ("sigma", "mu", "dg")}
+    normwise = max(abs(r[2] - r[3]) / scale[r[0]] for r in smooth)
+    print("FD_CALIBRATION_FP64_1e-8_30_steps " + json.dumps({"parameters": len(picks), "decisions_kept": len(smooth),
+                                                             "median_rel": rels[len(rels) // 2], "max_rel": rels[-1],
+                                                             "max_rel_to_largest_gradient": normwise}))
+    for r in smooth + jumps:
+        print(r)
+    assert len(jumps) == 0
+    assert rels[len(rels) // 2] <= 1e-3
+    assert normwise <= 1e-3
+    # (3)
+    ctx, R, state, sig, mu, dg = _setup(precision="fp64", interval=16, case=case, nsteps=case.nsteps)
+    rng = np.random.default_rng(6)
+    w = rng.standard_normal(G)
+    R.forward()
+    gs, gm, gd = R.backward(w)
+    assert R.adjoint_status == 0
+    ds = rng.standard_normal((G, G)); ds = (ds + ds.T) / 2; np.fill_diagonal(ds, 0)
+    dm = rng.standard_normal((G, G)); dm = (dm + dm.T) / 2; np.fill_diagonal(dm, 0)
+    dd = rng.standard_normal(G)
+    dV = R.tangent(ds, dm, dd)
+    iu = np.triu_indices(G, 1)
+    lhs = float(w @ dV)
+    rhs = float((gs[iu] * ds[iu]).sum() + (gm[iu] * dm[iu]).sum() + gd @ dd)
+    print("DOT_PRODUCT_CALIBRATION_200_STEPS", lhs, rhs, abs(lhs - rhs) / abs(lhs))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
