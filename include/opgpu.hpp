@@ -224,7 +224,15 @@ public:
     {
         Phi.check(opgpu_set_driving_force(Phi.ctx_, dG.data()), "DrivingForce::Force");
     }
-    /* $Average No: SkipAverage (src/DrivingForce.cpp:258-274); averaging is not part of this step. */
+    /* $Average / $Range / $Threshold of @DrivingForce (src/DrivingForce.cpp:129-133; Range <= 0 and
+     * Threshold <= 0 take the reference's defaults).  The reference's default is Yes. */
+    void SetAveraging(PhaseField& Phi, bool Averaging, int Range = 0, double Threshold = 0.0)
+    {
+        Phi.check(opgpu_set_averaging(Phi.ctx_, Averaging ? 1 : 0, Range, Threshold), "DrivingForce::ReadInput");
+    }
+    /* DrivingForce::Average (src/DrivingForce.cpp:242-256): with averaging on, SetWeights,
+     * CollectAverage and DistributeAverage run inside the fused step on the state it starts from;
+     * else SkipAverage (:258-274). */
     void Average(PhaseField&, const BoundaryConditions&) {}
     void MergePhaseFieldIncrements(PhaseField& Phi, InterfaceProperties&)
     {
