@@ -9,14 +9,17 @@
 //              the threshold, or the voxel's own tmp (0 when the pair is not above the threshold
 //              there: such a pair gets no driving force), then the tanh limiter of
 //              MergePhaseFieldIncrementsSR (:548-583).
-// Weights: PHASEFIELDS (the default, :59, :137); Threshold' = sqrt(t (1 - t)).  The sphere offsets
-// with Range - |d| > 0 are enumerated on the host in the reference's (x, y, z) loop order, so every
-// sum is formed in its order.  Compiled with --fmad=false.  The limiter's tanh is CUDA's here (the
-// averaged value differs per voxel), which can differ from the C library's in the last bit.
+// Weights: PHASEFIELDS (the default, :59, :137); Threshold' = sqrt(t (1 - t)).  A step with
+// averaging runs the per-voxel generic kernel, which reads the averaged force (pair_force).  The
+// sphere offsets with Range - |d| > 0 are enumerated on the host in the reference's (x, y, z) loop
+// order, so every sum is formed in its order.  Compiled with --fmad=false.  The limiter's tanh is
+// CUDA's here (the averaged value differs per voxel), which can differ from the C library's in the
+// last bit.
 //
-// Storage: every stored pair (a < b < c) of an interface voxel has a slot off[v] + pair_pos(a, b, c)
-// for tmp and for the limited average (compact, an exclusive scan per step); a voxel whose slots
-// would pass the capacity keeps the raw per-pair force and raises OPGPU_E_AVERAGE_SKIPPED.
+// Storage: every stored pair (a < b < c) of an interface voxel has a slot
+// off[v] + pair_pos(a, b, c) for tmp and for the limited average (compact, an exclusive scan per
+// step); a voxel whose slots would pass the capacity keeps the raw per-pair force and raises
+// OPGPU_E_AVERAGE_SKIPPED.
 #include <cfloat>
 #include <cstdint>
 

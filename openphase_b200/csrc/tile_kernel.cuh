@@ -682,15 +682,12 @@ __global__ void __launch_bounds__(128) list_compute_kernel(const __grid_constant
         // ---- driving force (interface voxels only) ----------------------------------------------
         if (p.use_dg && flag == 2)
         {
-            int c = 0;   // stored fields: the leading entries with nonzero values
-#pragma unroll
-            for (int k = 0; k < N; k++) c += val[k] != R(0) ? 1 : 0;
 #pragma unroll
             for (int i = 0; i < N; i++)
 #pragma unroll
                 for (int j = i + 1; j < N; j++)
                 {
-                    const double locdG = pair_force(p, a, v, c, i, j, g[i], g[j]);
+                    const double locdG = limited_force(p, a, g[i], g[j]);
                     double norm = sqrt((double)val[i] * (double)val[j]);
                     if (a.gstage[g[i]] == 1 || a.gstage[g[j]] == 1) norm += 1.0e-6;
                     const double dpsi = locdG * (double)(R)pair_mobility(p, a, g[i], g[j]) * norm * p.pref_df;
@@ -974,9 +971,11 @@ template <class R>
 int launch_step(const StepParams& p, const StepArrays& a, int k_slots, int variant, void* stream,
                 LaunchInfo* info)
 {
-    if (variant == kVariantGeneric || p.aniso)
+    if (variant == kVariantGeneric || p.aniso || a.df_lim)
     {
-        // anisotropic energies need the gradients of every list entry: the general path only
+        // anisotropic energies need the gradients of every list entry, and the averaged driving
+        // force is read per voxel pair: the per-voxel generic kernel only (the tiled kernels stay
+        // free of both)
         if (info) info->kernels += 1;
         return launch_step_generic<R>(p, a, k_slots, stream);
     }

@@ -206,7 +206,7 @@ __device__ void warp_voxel_step(const StepParams& p, const StepArrays& a, long l
         // ---- 3. driving force (interface voxels only) ----
         if (p.use_dg && flag == 2)
         {
-            const double locdG = pair_force(p, a, v, c, i, j, gi, gj);
+            const double locdG = limited_force(p, a, gi, gj);
             double norm = sqrt((double)vali * (double)valj);
             if (a.gstage[gi] == 1 || a.gstage[gj] == 1) norm += 1.0e-6;
             const double dpsi = locdG * (double)(R)pair_mobility(p, a, gi, gj) * norm * p.pref_df;

@@ -43,25 +43,20 @@ def test_averaging_matches_reference_fixture_and_oracle(name):
             assert r["non_borderline_mismatch_voxels"] == 0 and r["max_dphi"] <= TOL, (s, r)
 
 
-def test_averaging_larger_grid_tiled_and_generic():
+def test_averaging_larger_grid():
     case = Case(48, 40, 32, 14, seed=31, iwidth=5.0, dt=0.08, sigma=1.2, sigma_pairs=(0.8, 0.4), dg_scale=0.15,
                 average=True, name="average_48")
     state = case.initial_state()
     tiled = Context.from_case(case, precision="fp64", k_slots=16, state=state)
-    generic = Context.from_case(case, precision="fp64", k_slots=16, state=state)
-    generic.set_kernel_variant("generic")
     ora = Oracle(case, *state)
     plain = Context.from_case(case.with_(average=False), precision="fp64", k_slots=16, state=state)
     prev = 0
     for s in (1, 10, 30):
         tiled.step(case.dt, s - prev)
-        generic.step(case.dt, s - prev)
         plain.step(case.dt, s - prev)
         ora.step(s - prev)
         prev = s
-        a, b = tiled.download(), generic.download()
-        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.max(np.abs(a[2] - b[2])) <= 1e-12
-        r = compare_states(a, ora.state(positive_only=True), case.ngrains)
+        r = compare_states(tiled.download(), ora.state(positive_only=True), case.ngrains)
         assert r["non_borderline_mismatch_voxels"] == 0 and r["max_dphi"] <= TOL, (s, r)
     # averaging is not a rounding-level change: pairs far from their interface core lose their force
     r = compare_states(tiled.download(), plain.download(), case.ngrains)
