@@ -312,6 +312,13 @@ int64_t  opgpu_plane_bytes(opgpu_ctx* ctx);
 /* Copy x-plane x of the current state to / from a device buffer of opgpu_plane_bytes bytes. */
 uint32_t opgpu_pack_plane(opgpu_ctx* ctx, int32_t x, void* dev_buf);
 uint32_t opgpu_unpack_plane(opgpu_ctx* ctx, int32_t x, const void* dev_buf);
+/* Stream-ordered slab calls (enable != 0): opgpu_pack_plane, opgpu_unpack_plane,
+ * opgpu_volume_recount, opgpu_volume_accumulator, opgpu_step_partial and opgpu_step_complete only
+ * enqueue their work on the context's stream (opgpu_stream) and return; the caller orders its own
+ * streams against it (e.g. events) before it reads or writes the device buffers involved, and
+ * reads the accumulated soft status with opgpu_sync.  Default (0): each call returns with its work
+ * done.  No reference counterpart. */
+uint32_t opgpu_set_stream_ordered(opgpu_ctx* ctx, int32_t enable);
 /* Recompute the grain-volume accumulator from the window planes of the current state. */
 uint32_t opgpu_volume_recount(opgpu_ctx* ctx);
 /* One step whose grain update is deferred: the window's volume sums stay in the accumulator. */

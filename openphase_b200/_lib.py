@@ -133,6 +133,7 @@ _SIGS = {
     "opgpu_unpack_plane": (C.c_uint32, [_P, C.c_int32, _P]),
     "opgpu_volume_recount": (C.c_uint32, [_P]),
     "opgpu_step_partial": (C.c_uint32, [_P, C.c_double]),
+    "opgpu_set_stream_ordered": (C.c_uint32, [_P, C.c_int32]),
     "opgpu_volume_accumulator": (C.c_uint32, [_P, _P]),
     "opgpu_step_complete": (C.c_uint32, [_P, _P, C.c_int32]),
     "opgpu_uniform": (C.c_double, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),

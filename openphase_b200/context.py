@@ -271,6 +271,10 @@ class Context:
     def unpack_plane(self, x: int, dev_ptr: int):
         _check(lib().opgpu_unpack_plane(self.h, int(x), C.c_void_p(dev_ptr)), self.h, "unpack_plane")
 
+    def set_stream_ordered(self, enable: bool):
+        """Slab calls only enqueue on the context's stream; the caller orders its streams."""
+        _check(lib().opgpu_set_stream_ordered(self.h, int(enable)), self.h, "set_stream_ordered")
+
     def volume_recount(self):
         _check(lib().opgpu_volume_recount(self.h), self.h, "volume_recount")
 

@@ -97,6 +97,7 @@ struct opgpu_ctx {
     double timed_classify_ms = 0.0;
     long long kernel_launches = 0;   // kernels of this library launched on the context's stream
     int8_t* noalloc_scratch = nullptr;   // device address of the allocation-free flag scratch
+    bool stream_ordered = false;         // slab calls enqueue only (the caller orders its streams)
     // driving-force averaging ($Average Yes)
     bool averaging = false;
     int avg_range = 0;
@@ -1794,7 +1795,7 @@ static uint32_t plane_copy(opgpu_ctx* ctx, int32_t x, void* buf, bool pack)
         CK(cudaMemcpy2DAsync(i, N * 2, bi, P * 2, P * 2, K, kind, ctx->stream));
         CK(cudaMemcpy2DAsync(v, N * ctx->rsz, bv, P * ctx->rsz, P * ctx->rsz, K, kind, ctx->stream));
     }
-    CK(cudaStreamSynchronize(ctx->stream));
+    if (!ctx->stream_ordered) CK(cudaStreamSynchronize(ctx->stream));
     return OPGPU_OK;
 }
 
@@ -1812,7 +1813,7 @@ extern "C" uint32_t opgpu_volume_recount(opgpu_ctx* ctx)
                               ctx->d_vol_acc, ctx->stream))
         return fail(ctx, OPGPU_E_CUDA, "opgpu_volume_recount: launch");
     ctx->kernel_launches++;
-    CK(cudaStreamSynchronize(ctx->stream));
+    if (!ctx->stream_ordered) CK(cudaStreamSynchronize(ctx->stream));
     return OPGPU_OK;
 }
 
@@ -1821,7 +1822,15 @@ extern "C" uint32_t opgpu_step_partial(opgpu_ctx* ctx, double dt)
     if (ctx && ctx->averaging)
         return fail(ctx, OPGPU_E_INVALID, "opgpu_step_partial: a slab holds one halo plane; averaging needs Range planes");
     if (uint32_t r = enqueue_steps(ctx, dt, 1, true)) return r;
+    if (ctx->stream_ordered) return OPGPU_OK;   // the soft status accumulates for opgpu_sync
     return opgpu_sync(ctx);
+}
+
+extern "C" uint32_t opgpu_set_stream_ordered(opgpu_ctx* ctx, int32_t enable)
+{
+    if (uint32_t r = require(ctx, ctx != nullptr, "opgpu_set_stream_ordered: no context")) return r;
+    ctx->stream_ordered = enable != 0;
+    return OPGPU_OK;
 }
 
 extern "C" uint32_t opgpu_volume_accumulator(opgpu_ctx* ctx, double* dev_dst)
@@ -1829,7 +1838,7 @@ extern "C" uint32_t opgpu_volume_accumulator(opgpu_ctx* ctx, double* dev_dst)
     if (uint32_t r = require(ctx, ctx && ctx->G > 0, "opgpu_volume_accumulator: no grains")) return r;
     if (!dev_dst) return fail(ctx, OPGPU_E_INVALID, "opgpu_volume_accumulator: NULL buffer");
     CK(cudaMemcpyAsync(dev_dst, ctx->d_vol_acc, (size_t)ctx->G * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    if (!ctx->stream_ordered) CK(cudaStreamSynchronize(ctx->stream));
     return OPGPU_OK;
 }
 
@@ -1847,6 +1856,7 @@ extern "C" uint32_t opgpu_step_complete(opgpu_ctx* ctx, const double* dev_src, i
         ctx->d_maxvol, ctx->d_refvol, ctx->d_vr, ctx->d_exist, ctx->d_gstage, ctx->d_counters, initial ? 0 : 1);
     CK(cudaGetLastError());
     ctx->kernel_launches += initial ? 2 : 1;
+    if (ctx->stream_ordered) return OPGPU_OK;   // the soft status accumulates for opgpu_sync
     const uint32_t st = read_status(ctx);
     if (st & OPGPU_E_CUDA) return st;
     return st & OPGPU_SOFT_MASK;

@@ -12,7 +12,12 @@ The reference does the same with MPI: halo cells (include/BoundaryConditions.h:2
 all-reduce of the grain volumes (src/PhaseField.cpp:854-892).
 
 Communication goes through a `comm` object with exchange(send_lo, send_hi) -> (recv_lo, recv_hi)
-and allreduce(tensor): `DistComm` uses torch.distributed (NCCL on GPUs, gloo on CPU tensors).
+and allreduce(tensor): `DistComm` uses torch.distributed (NCCL on the device buffers; with gloo the
+buffers are staged through host memory).  The context runs stream-ordered (its slab calls only
+enqueue work on its own stream): the stepper makes torch's stream wait for the context's stream
+before a buffer is sent or reduced, and the context's stream wait for torch's before a received
+buffer is used, so no step synchronises the host except for the staging of a gloo exchange and the
+status read at the end of `step`.
 """
 from __future__ import annotations
 
@@ -57,14 +62,24 @@ class DistComm:
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
 
+    @property
+    def staged(self) -> bool:
+        """gloo moves host tensors only: device buffers go through host memory."""
+        return self.dist.get_backend(self.group) == "gloo"
+
     def exchange(self, send_lo, send_hi):
         """send_lo (first interior plane) goes to rank-1 as its upper halo, send_hi (last interior
         plane) to rank+1 as its lower halo.  Two phases, each with one send and one receive per
-        neighbour, so that the messages cannot pair up wrongly when both neighbours are one rank."""
+        neighbour, so that the messages cannot pair up wrongly when both neighbours are one rank.
+        The operations run on torch's current stream (which the caller has ordered after the
+        packing); the received buffers are ready on that stream when this returns."""
         import torch
         if self.world == 1:
             return send_hi.clone(), send_lo.clone()
         d = self.dist
+        dev = send_lo.device
+        if self.staged and send_lo.is_cuda:
+            send_lo, send_hi = send_lo.cpu(), send_hi.cpu()
         lo, hi = (self.rank - 1) % self.world, (self.rank + 1) % self.world
         recv_lo, recv_hi = torch.empty_like(send_lo), torch.empty_like(send_hi)
         for op in d.batch_isend_irecv([d.P2POp(d.isend, send_hi, hi, self.group),
@@ -73,21 +88,20 @@ class DistComm:
         for op in d.batch_isend_irecv([d.P2POp(d.isend, send_lo, lo, self.group),
                                        d.P2POp(d.irecv, recv_hi, hi, self.group)]):
             op.wait()
-        self._settle(recv_lo)
+        if recv_lo.device != dev:
+            recv_lo, recv_hi = recv_lo.to(dev), recv_hi.to(dev)
         return recv_lo, recv_hi
 
     def allreduce(self, t):
+        """In place on torch's current stream (through host memory with gloo)."""
         if self.world > 1:
-            self.dist.all_reduce(t, group=self.group)
-            self._settle(t)
+            if self.staged and t.is_cuda:
+                h = t.cpu()
+                self.dist.all_reduce(h, group=self.group)
+                t.copy_(h)
+            else:
+                self.dist.all_reduce(t, group=self.group)
         return t
-
-    @staticmethod
-    def _settle(t):
-        """The context's kernels run on their own stream: wait until the collective has landed."""
-        if t.is_cuda:
-            import torch
-            torch.cuda.current_stream(t.device).synchronize()
 
 
 class SlabStepper:
@@ -117,34 +131,58 @@ class SlabStepper:
         counts, idx, val = state if state is not None else case.initial_state()
         ctx.upload(*local_lists(counts, idx, val, (case.nx, case.ny, case.nz), self.x0, self.x1))
         ctx.finalize_initialization()
+        ctx.set_stream_ordered(True)
         self.ctx = ctx
         self.torch_device = torch.device("cuda", device)
+        self.ctx_stream = torch.cuda.ExternalStream(ctx.stream, device=self.torch_device)
         nb = ctx.plane_bytes()
         self.send_lo = torch.empty(nb, dtype=torch.uint8, device=self.torch_device)
         self.send_hi = torch.empty(nb, dtype=torch.uint8, device=self.torch_device)
         self.acc = torch.empty(case.ngrains, dtype=torch.float64, device=self.torch_device)
 
-    # ---- the three phases of a step
+    # ---- stream order between the context's stream and torch's current stream
+    def to_torch(self):
+        """Work enqueued on the context's stream so far comes before torch's next operations."""
+        import torch
+        torch.cuda.current_stream(self.torch_device).wait_stream(self.ctx_stream)
+
+    def from_torch(self):
+        """torch's operations so far come before the context's next work."""
+        import torch
+        self.ctx_stream.wait_stream(torch.cuda.current_stream(self.torch_device))
+
+    # ---- the three phases of a step (each returns with its buffers ready on torch's stream)
     def pack(self):
+        self.from_torch()   # the previous exchange has read the send buffers
         self.ctx.pack_plane(1, self.send_lo.data_ptr())
         self.ctx.pack_plane(self.nxl - 2, self.send_hi.data_ptr())
+        self.to_torch()
         return self.send_lo, self.send_hi
 
     def unpack(self, recv_lo, recv_hi):
+        self.from_torch()
         self.ctx.unpack_plane(0, recv_lo.data_ptr())
         self.ctx.unpack_plane(self.nxl - 1, recv_hi.data_ptr())
+        self._keep = (recv_lo, recv_hi)   # alive until the context's stream has read them
 
     def step_partial(self, dt) -> int:
         st = self.ctx.step_partial(dt)
         self.ctx.volume_accumulator(self.acc.data_ptr())
+        self.to_torch()
         return st
 
     def recount(self):
         self.ctx.volume_recount()
         self.ctx.volume_accumulator(self.acc.data_ptr())
+        self.to_torch()
 
     def complete(self, total, initial=False) -> int:
+        self.from_torch()
         return self.ctx.step_complete(total.data_ptr(), initial)
+
+    def sync(self) -> int:
+        """Wait for the context's stream; the soft status its steps raised."""
+        return self.ctx.sync()
 
     def interior(self):
         """Ragged lists of the interior planes (global planes x0 .. x1-1)."""
@@ -160,16 +198,18 @@ def initialize(stepper: SlabStepper, comm):
     """Global grain volumes of the initial state (FinalizeInitialization's update)."""
     stepper.recount()
     comm.allreduce(stepper.acc)
-    return stepper.complete(stepper.acc, initial=True)
+    stepper.complete(stepper.acc, initial=True)
+    return stepper.sync()
 
 
 def step(stepper: SlabStepper, comm, dt: float, nsteps: int = 1) -> int:
-    status = 0
+    """nsteps slab steps; returns the soft status they raised (one host synchronisation at the end,
+    besides the staging of a gloo exchange)."""
     for _ in range(nsteps):
         lo, hi = stepper.pack()
         rlo, rhi = comm.exchange(lo, hi)
         stepper.unpack(rlo, rhi)
-        status |= stepper.step_partial(dt)
+        stepper.step_partial(dt)
         comm.allreduce(stepper.acc)
-        status |= stepper.complete(stepper.acc)
-    return status
+        stepper.complete(stepper.acc)
+    return stepper.sync()
