@@ -21,7 +21,7 @@
 //   adjoint_worklist_kernel the voxels of the general-path worklist (general gather);
 //   adjoint_bulk_kernel  bulk voxels: the adjoint passes through
 //   adjoint_gather_kernel adjoint of the stored values at t: own part plus the transposed stencil
-//                        over the neighbours' Laplacian adjoints
+//                        over the neighbours' Laplacian adjoints (tiled like the classify kernel)
 // Compiled with --fmad=false so that the recomputed FP64 arithmetic repeats the forward's.
 #include <cfloat>
 #include <cmath>
@@ -29,6 +29,7 @@
 
 #include "adjoint.h"
 #include "step_kernel.cuh"
+#include "tile_kernel.cuh"
 
 namespace opgpu {
 
@@ -935,27 +936,147 @@ __global__ void __launch_bounds__(64) adjoint_worklist_kernel(const __grid_const
 }
 
 // lambda_t(u, s) = own part + sum_q w_q * (adjoint of the Laplacian of grain g_s at u - d_q)
-__global__ void adjoint_gather_kernel(const __grid_constant__ StepParams p, const uint8_t* __restrict__ cnt,
-                                      const int16_t* __restrict__ idx, const AdjArrays aa, double* __restrict__ lam0)
+//
+// The adjoints of the Laplacians form ragged lists (lcnt, lidx, llam) in the slot-planar layout of
+// a state, so the transposed stencil is evaluated like the forward Laplacians: the classify
+// kernel's plane loader brings three x-planes of those lists into dense per-slot planes, and every
+// entry of the centre voxel sums w_q * dense[slot(g_s)][u - d_q] in stencil order (absent grains
+// read zeros, which leave the sum unchanged).  Voxels next to a list grain without a window slot
+// take the same sum from global memory.
+
+// Neighbour u - d without indexing the offset arrays by a runtime value (selects only).
+__device__ __forceinline__ long long nb_back(const Neighbourhood& nb, const signed char* d)
+{
+    const long long x = d[0] > 0 ? nb.X[0] : (d[0] < 0 ? nb.X[2] : nb.X[1]);
+    const long long y = d[1] > 0 ? nb.Y[0] : (d[1] < 0 ? nb.Y[2] : nb.Y[1]);
+    const long long z = d[2] > 0 ? nb.Z[0] : (d[2] < 0 ? nb.Z[2] : nb.Z[1]);
+    return x + y + z;
+}
+
+__device__ __forceinline__ double gather_global(const StepParams& p, const AdjArrays& aa, const Neighbourhood& nb,
+                                                int g, double l)
 {
     const long long N = p.n;
-    const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= N) return;
-    const Neighbourhood nb(p, u);
-    const int c = cnt[u];
-    for (int s = 0; s < c; s++)
+    for (int q = 0; q < p.ns; q++)
     {
-        const int g = idx[s * N + u];
-        double l = aa.lam_local[s * N + u];
-        for (int q = 0; q < p.ns; q++)
-        {
-            const long long v = nb.at(-p.lap_d[q][0], -p.lap_d[q][1], -p.lap_d[q][2]);
-            const int lc = aa.lcnt[v];
-            for (int k = 0; k < lc; k++)
-                if (aa.lidx[k * N + v] == g) { l += p.lap_w[q] * aa.llam[k * N + v]; break; }
-        }
-        lam0[s * N + u] = l;
+        const long long v = nb_back(nb, p.lap_d[q]);
+        const int lc = aa.lcnt[v];
+        for (int k = 0; k < lc; k++)
+            if (aa.lidx[k * N + v] == g) { l += p.lap_w[q] * aa.llam[k * N + v]; break; }
     }
+    return l;
+}
+
+template <int KS, int NS>
+__global__ void __launch_bounds__(kTileZ * kTileTY)
+adjoint_gather_kernel(const __grid_constant__ StepParams p, const StepArrays la, const uint8_t* __restrict__ cnt,
+                      const int16_t* __restrict__ idx, const AdjArrays aa, double* __restrict__ lam0, int xchunk)
+{
+    constexpr int TY = kTileTY;
+    using Geo = TileGeom<TY>;
+    using Smem = TileSmem<double, KS, TY>;
+    constexpr int NT = Geo::NT;
+    constexpr int kC = Geo::kCols;
+    constexpr int kSlots = WindowSlots<double>::value;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+
+    const int tz = threadIdx.x, ty = threadIdx.y, t = ty * kTileZ + tz;
+    const int z0 = blockIdx.x * kTileZ, y0 = blockIdx.y * TY, x0 = blockIdx.z * xchunk;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int x1 = min(x0 + xchunk, nx);
+    const long long N = p.n;
+    const long long plane = (long long)ny * nz;
+    const int z = z0 + tz, y = y0 + ty;
+    const bool inside = (z < nz) && (y < ny);
+
+    for (int i = t; i < kSlots * 3 * Geo::kRecs; i += NT) (&S.dense[0][0][0])[i] = 0.0;
+    for (int i = t; i < 3 * Geo::kRecs; i += NT) (&S.word[0][0])[i] = 0u;
+    if (t < kSlots) { S.grain_of[t] = -1; S.lastpos[t] = -1000; }
+    if (t < kSlotHash) S.hkey[t] = -1;
+    if (t < 32) S.pending[t] = -1;
+    if (t == 0) S.tomb = 0;
+    int cr[PlaneRegs<TY>::kPer];
+    prefetch_counts<TY>(p, la, x0 == 0 ? nx - 1 : x0 - 1, y0, z0, t, cr);
+    __syncthreads();
+
+    const int rec0 = (ty + 1) * kC + (tz + 1);
+    const int nj = (x1 - x0) + 2;
+    for (int j = 0; j < nj; j++)
+    {
+        int xp = x0 - 1 + j;
+        xp = xp < 0 ? xp + nx : (xp >= nx ? xp - nx : xp);
+        if (j > 0) __syncthreads();
+        load_plane(p, la, S, j % 3, xp, j - 1, y0, z0, t, cr);
+        __syncthreads();
+        if (j < 2 || !inside) continue;
+        const int x = x0 + j - 2;
+        const int sl0 = (j - 2) % 3, sl1 = (j - 1) % 3, sl2 = j % 3;
+        const long long u = (long long)x * plane + (long long)y * nz + z;
+        // a list grain of a stencil neighbour without a window slot: the global sum
+        bool crowded = false;
+#pragma unroll
+        for (int q = 0; q < NS; q++)
+        {
+            const int dx = stencil_dx<NS>(q);
+            const int pl = dx > 0 ? sl0 : (dx < 0 ? sl2 : sl1);
+            const int r = rec0 - stencil_dy<NS>(q) * kC - stencil_dz<NS>(q);
+            crowded |= ((S.word[pl][r] >> 30) & 1u) != 0u;
+        }
+        const int c = cnt[u];
+        for (int s = 0; s < c; s++)
+        {
+            const int g = idx[s * N + u];
+            double l = aa.lam_local[s * N + u];
+            if (crowded)
+            {
+                const Neighbourhood nb(p, u);
+                l = gather_global(p, aa, nb, g, l);
+            }
+            else
+            {
+                const int k = find_slot(S.hkey, S.hslot, g);
+                if (k >= 0)
+                {
+#pragma unroll
+                    for (int q = 0; q < NS; q++)
+                    {
+                        const int dx = stencil_dx<NS>(q);
+                        const int pl = dx > 0 ? sl0 : (dx < 0 ? sl2 : sl1);
+                        const int r = rec0 - stencil_dy<NS>(q) * kC - stencil_dz<NS>(q);
+                        l += p.lap_w[q] * S.dense[k][pl][r];
+                    }
+                }
+            }
+            lam0[s * N + u] = l;
+        }
+    }
+}
+
+template <int KS, int NS>
+static int launch_gather_ns(const StepParams& p, const StepArrays& a, const AdjArrays& aa, double* lam0, cudaStream_t s)
+{
+    using Smem = TileSmem<double, KS, kTileTY>;
+    int xchunk = 0, gz = 0, gy = 0, gx = 0;
+    tiled_geometry(p.nx, p.ny, p.nz, &xchunk, &gz, &gy, &gx);
+    StepArrays la = a;   // the plane loader reads the lists of the Laplacian adjoints
+    la.cnt_in = aa.lcnt;
+    la.idx_in = aa.lidx;
+    la.val_in = aa.llam;
+    auto kern = adjoint_gather_kernel<KS, NS>;
+    const size_t smem = sizeof(Smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    kern<<<dim3(gz, gy, gx), dim3(kTileZ, kTileTY), smem, s>>>(p, la, a.cnt_in, a.idx_in, aa, lam0, xchunk);
+    return (int)cudaGetLastError();
+}
+
+template <int KS>
+static int launch_gather(const StepParams& p, const StepArrays& a, const AdjArrays& aa, double* lam0, cudaStream_t s)
+{
+    if (p.ns == 27) return launch_gather_ns<KS, 27>(p, a, aa, lam0, s);
+    if (p.ns == 7) return launch_gather_ns<KS, 7>(p, a, aa, lam0, s);
+    return -1;
 }
 
 __global__ void lambda_init_kernel(long long N, const uint8_t* __restrict__ cnt, const int16_t* __restrict__ idx,
@@ -984,9 +1105,13 @@ int launch_tlm_step(const StepParams& p, const StepArrays& a, const AdjArrays& a
 
 constexpr int kAdjListBlocks = 148 * 8;   // blocks of each per-length adjoint kernel
 
+// The worklist kernel (few voxels, each a long serial chain) runs on the side stream, launched
+// first, so that it overlaps the list-length kernels instead of adding its latency after them.
 template <class R, int KS>
-static void adjoint_kernels(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int nblocks, cudaStream_t s)
+static void adjoint_kernels(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int nblocks, cudaStream_t s,
+                            cudaStream_t side)
 {
+    adjoint_worklist_kernel<R, KS><<<148 * 4, 64, 0, side>>>(p, a, aa);
     adjoint_list_kernel<R, 2, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
     adjoint_list_kernel<R, 3, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
     adjoint_list_kernel<R, 4, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
@@ -994,25 +1119,44 @@ static void adjoint_kernels(const StepParams& p, const StepArrays& a, const AdjA
     adjoint_list_kernel<R, 6, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
     adjoint_list_kernel<R, 7, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
     adjoint_list_kernel<R, 8, KS><<<kAdjListBlocks, 128, 0, s>>>(p, a, aa, nblocks);
-    adjoint_worklist_kernel<R, KS><<<148 * 4, 64, 0, s>>>(p, a, aa);
 }
 
 int launch_adjoint_step(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int k_slots, bool fp32,
-                        int nblocks, double* lam0, void* stream)
+                        int nblocks, double* lam0, void* stream, const AdjStreams& fork)
 {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStream_t side = fork.side ? static_cast<cudaStream_t>(fork.side) : s;
     adjoint_bulk_kernel<<<grid_of(p.n, 256), 256, 0, s>>>(p, a.cnt_in, aa);
+    cudaError_t e;
+    if (side != s)
+    {
+        if ((e = cudaEventRecord(static_cast<cudaEvent_t>(fork.ev_fork), s)) != cudaSuccess) return (int)e;
+        if ((e = cudaStreamWaitEvent(side, static_cast<cudaEvent_t>(fork.ev_fork), 0)) != cudaSuccess) return (int)e;
+    }
     switch (k_slots * 2 + (fp32 ? 1 : 0))
     {
-        case 16: adjoint_kernels<double, 8>(p, a, aa, nblocks, s); break;
-        case 17: adjoint_kernels<float, 8>(p, a, aa, nblocks, s); break;
-        case 24: adjoint_kernels<double, 12>(p, a, aa, nblocks, s); break;
-        case 25: adjoint_kernels<float, 12>(p, a, aa, nblocks, s); break;
-        case 32: adjoint_kernels<double, 16>(p, a, aa, nblocks, s); break;
-        case 33: adjoint_kernels<float, 16>(p, a, aa, nblocks, s); break;
+        case 16: adjoint_kernels<double, 8>(p, a, aa, nblocks, s, side); break;
+        case 17: adjoint_kernels<float, 8>(p, a, aa, nblocks, s, side); break;
+        case 24: adjoint_kernels<double, 12>(p, a, aa, nblocks, s, side); break;
+        case 25: adjoint_kernels<float, 12>(p, a, aa, nblocks, s, side); break;
+        case 32: adjoint_kernels<double, 16>(p, a, aa, nblocks, s, side); break;
+        case 33: adjoint_kernels<float, 16>(p, a, aa, nblocks, s, side); break;
         default: return -1;
     }
-    adjoint_gather_kernel<<<grid_of(p.n, 128), 128, 0, s>>>(p, a.cnt_in, a.idx_in, aa, lam0);
+    if (side != s)
+    {
+        if ((e = cudaEventRecord(static_cast<cudaEvent_t>(fork.ev_join), side)) != cudaSuccess) return (int)e;
+        if ((e = cudaStreamWaitEvent(s, static_cast<cudaEvent_t>(fork.ev_join), 0)) != cudaSuccess) return (int)e;
+    }
+    int rc = -1;
+    switch (k_slots)
+    {
+        case 8:  rc = launch_gather<8>(p, a, aa, lam0, s); break;
+        case 12: rc = launch_gather<12>(p, a, aa, lam0, s); break;
+        case 16: rc = launch_gather<16>(p, a, aa, lam0, s); break;
+        default: return -1;
+    }
+    if (rc != 0) return rc;
     return (int)cudaGetLastError();
 }
 

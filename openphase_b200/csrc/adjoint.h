@@ -36,8 +36,15 @@ int launch_tlm_step(const StepParams& p, const StepArrays& a, const AdjArrays& a
 // and its adjoint; the classify kernel has just run on the state before the step (its work
 // records, buckets and worklist in a; nblocks its block count).  Writes the adjoint of the state
 // before the step to lam0 and accumulates the parameter gradients.
+// A side stream with a fork and a join event (cudaEvent_t, timing disabled) for the worklist
+// kernel; side == nullptr runs everything on the main stream.
+struct AdjStreams {
+    void* side;
+    void* ev_fork;
+    void* ev_join;
+};
 int launch_adjoint_step(const StepParams& p, const StepArrays& a, const AdjArrays& aa, int k_slots, bool fp32,
-                        int nblocks, double* lam0, void* stream);
+                        int nblocks, double* lam0, void* stream, const AdjStreams& fork);
 // lam[s][v] = dLdV[idx[s][v]] on the stored entries (adjoint of a loss on the grain volumes).
 int launch_lambda_init(long long n, const uint8_t* cnt, const int16_t* idx, const double* dLdV, double* lam,
                        void* stream);

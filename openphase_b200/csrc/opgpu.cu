@@ -25,6 +25,9 @@ struct opgpu_ctx {
     opgpu_grid grid{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    void* adj_side = nullptr;            // adjoint: side stream of the worklist kernel, fork / join events
+    void* adj_fork = nullptr;
+    void* adj_join = nullptr;
     std::string err;
     long long n = 0;
     int K = 8;
@@ -620,6 +623,9 @@ extern "C" uint32_t opgpu_destroy(opgpu_ctx* ctx)
     dfree(ctx->d_lam_local); dfree(ctx->d_lcnt); dfree(ctx->d_lidx); dfree(ctx->d_llam);
     dfree(ctx->d_gsig); dfree(ctx->d_gmu); dfree(ctx->d_gdg);
     dfree(ctx->d_tsig); dfree(ctx->d_tmu); dfree(ctx->d_tdg); dfree(ctx->d_tvol);
+    if (ctx->adj_side) cudaStreamDestroy(static_cast<cudaStream_t>(ctx->adj_side));
+    if (ctx->adj_fork) cudaEventDestroy(static_cast<cudaEvent_t>(ctx->adj_fork));
+    if (ctx->adj_join) cudaEventDestroy(static_cast<cudaEvent_t>(ctx->adj_join));
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return OPGPU_OK;
@@ -1507,6 +1513,17 @@ uint32_t ensure_adjoint(opgpu_ctx* ctx)
     CK(dalloc(&ctx->d_gsig, G * G));
     CK(dalloc(&ctx->d_gmu, G * G));
     CK(dalloc(&ctx->d_gdg, G));
+    if (!ctx->adj_side)
+    {
+        cudaStream_t side;
+        cudaEvent_t ef, ej;
+        CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        ctx->adj_side = side;
+        CK(cudaEventCreateWithFlags(&ef, cudaEventDisableTiming));
+        ctx->adj_fork = ef;
+        CK(cudaEventCreateWithFlags(&ej, cudaEventDisableTiming));
+        ctx->adj_join = ej;
+    }
     ctx->adjoint_ready = true;
     return OPGPU_OK;
 }
@@ -1647,7 +1664,8 @@ extern "C" uint32_t opgpu_adjoint_step(opgpu_ctx* ctx, int32_t slot, double dt)
     CK(cudaMemsetAsync(ctx->d_vol_acc, 0, (size_t)ctx->G * sizeof(double), ctx->stream));
     CK(cudaMemsetAsync(ctx->d_counters, 0, 3 * sizeof(unsigned long long), ctx->stream));   // wide, entries in/out
     CK(cudaMemsetAsync(ctx->d_counters + kCntCrowdedLast, 0, sizeof(unsigned long long), ctx->stream));
-    if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, nblocks, lam0, ctx->stream))
+    const AdjStreams fork{ctx->adj_side, ctx->adj_fork, ctx->adj_join};
+    if (launch_adjoint_step(sp, a, aa, ctx->K, ctx->fp32 != 0, nblocks, lam0, ctx->stream, fork))
         return fail(ctx, OPGPU_E_CUDA, "opgpu_adjoint_step: launch");
     ctx->kernel_launches += 12;
     ctx->lam_cur = 1 - ctx->lam_cur;
