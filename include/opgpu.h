@@ -82,7 +82,8 @@ typedef struct opgpu_model {
     /* Anisotropic interface energy (InterfaceEnergyModel.h:78-94, 325-345; InterfaceProperties.cpp:
      * 617-673); any may be NULL (all ISO, all phases solid). */
     const int32_t* energy_model;   /* [P*P] 0 = ISO, 1 = CUBIC, 2 = DISORIENTATION, 3 = HEXBOETTGER,
-                                      4 = HEXSUN, 5 = HEXYANG, 6 = FACETED ($EnergyModel_a_b;
+                                      4 = HEXSUN, 5 = HEXYANG, 6 = FACETED, 7 = FACETEDEXP
+                                      ($EnergyModel_a_b;
                                       DISORIENTATION: InterfaceEnergyModel.h:303-323, the energy of
                                       a grain pair from the cubic disorientation of the two grains'
                                       orientations (opgpu_set_orientations), tabulated per grain pair;
@@ -99,17 +100,28 @@ typedef struct opgpu_model {
      * facet_start[q] .. facet_start[q+1]-1 of facet_data, 5 doubles each: h, k, l ($Facet_a_b_n),
      * SigmaF ($SigmaF_a_b_n), EpsilonEF ($EpsilonEF_a_b_n); facet_family[q] = 1 makes every facet
      * stand for its family of index permutations ($NfacetFamilies_a_b), 0 for itself ($Nfacets_a_b).
-     * Energy = mean SigmaF, MaxEnergy = max SigmaF.  All three may be NULL without FACETED pairs. */
+     * Energy = mean SigmaF, MaxEnergy = max SigmaF.  All three may be NULL without FACETED pairs.
+     * FACETEDEXP (InterfaceEnergyModel.h:248-295, 389-413) reads the same table with the last two
+     * columns EpsilonEF ($EpsilonEF_a_b_n) and PowerEF ($PowerEF_a_b_n, >= 2); its Energy and
+     * MaxEnergy are $Sigma_a_b (sigma[q]). */
     const int32_t* facet_start;    /* [P*P+1]                                                      */
     const double* facet_data;      /* [facet_start[P*P]*5]                                         */
     const int32_t* facet_family;   /* [P*P]                                                        */
     /* Anisotropic interface mobility (InterfaceMobilityModel.h:71-113, 210-265; InterfaceProperties.cpp:
-     * 680-707): per phase pair 0 = ISO, 1 = CUBIC, 3 = HEXBOETTGER, 4 = HEXSUN, 5 = HEXYANG
-     * ($MobilityModel_a_b) and Epsilon1..4 ($EpsilonM_a_b; HEXSUN $EpsilonM20/40/60/66_a_b; HEXYANG
+     * 680-707): per phase pair 0 = ISO, 1 = CUBIC, 3 = HEXBOETTGER, 4 = HEXSUN, 5 = HEXYANG,
+     * 6 = FACETED ($MobilityModel_a_b) and Epsilon1..4 ($EpsilonM_a_b; HEXSUN $EpsilonM20/40/60/66_a_b; HEXYANG
      * $EpsilonM1/2/3_a_b).  Per voxel and pair the model is summed over the solid grains whose value
      * is neither 0 nor 1 (not averaged, as in the reference), else Mobility.  NULL: all ISO.      */
     const int32_t* mobility_model; /* [P*P]                                                        */
     const double* mobility_eps;    /* [P*P*4]                                                      */
+    /* FACETED mobility (mobility model 6; InterfaceMobilityModel.h:165-208, 266-287): the facets of
+     * phase pair q are rows mobility_facet_start[q] .. [q+1]-1 of mobility_facet_data, 5 doubles
+     * each: h, k, l ($Facet_a_b_n), MuF ($MuF_a_b_n), EpsilonMF ($EpsilonMF_a_b_n);
+     * mobility_facet_family as facet_family.  The model reads no $Mu: its Mobility, used where no
+     * solid grain of the pair counts, is 0 as in the reference.  NULL without such pairs.        */
+    const int32_t* mobility_facet_start;   /* [P*P+1]                                              */
+    const double* mobility_facet_data;     /* [mobility_facet_start[P*P]*5]                        */
+    const int32_t* mobility_facet_family;  /* [P*P]                                                */
 } opgpu_model;
 
 typedef struct opgpu_stats {

@@ -65,7 +65,9 @@ class Model(C.Structure):
                 ("cubic_eps", C.POINTER(C.c_double)), ("phase_solid", C.POINTER(C.c_int32)),
                 ("model_eps", C.POINTER(C.c_double)), ("facet_start", C.POINTER(C.c_int32)),
                 ("facet_data", C.POINTER(C.c_double)), ("facet_family", C.POINTER(C.c_int32)),
-                ("mobility_model", C.POINTER(C.c_int32)), ("mobility_eps", C.POINTER(C.c_double))]
+                ("mobility_model", C.POINTER(C.c_int32)), ("mobility_eps", C.POINTER(C.c_double)),
+                ("mobility_facet_start", C.POINTER(C.c_int32)), ("mobility_facet_data", C.POINTER(C.c_double)),
+                ("mobility_facet_family", C.POINTER(C.c_int32))]
 
 
 class Stats(C.Structure):

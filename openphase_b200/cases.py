@@ -60,8 +60,11 @@ class Case:
     hex_eps: tuple = (0.0, 0.0, 0.0)           # Epsilon2..4 of the HEX model (Epsilon1: phase_cubic_eps)
     facets: tuple = ()                         # FACETED in place of CUBIC: (h, k, l, SigmaF, EpsilonEF) each
     facet_families: bool = True                # every facet stands for its family of permutations
-    mobility_model: str = ""                   # CUBIC / HEXBOETTGER / HEXSUN / HEXYANG mobility on the pairs
+    facet_exp: bool = False                    # FACETEDEXP in place of FACETED: facets are (h, k, l, EpsilonEF, PowerEF)
+    mobility_model: str = ""                   # CUBIC / HEXBOETTGER / HEXSUN / HEXYANG / FACETED mobility on the pairs
     mobility_eps: tuple = (0.0, 0.0, 0.0, 0.0)  # with anisotropic energy (phase_cubic_eps != 0): Epsilon1..4
+    mobility_facets: tuple = ()                # FACETED mobility: (h, k, l, MuF, EpsilonMF) each
+    mobility_facet_families: bool = True
 
     @property
     def n(self) -> int:
@@ -93,14 +96,17 @@ class Case:
         e = self.cubic_eps()
         if e is None:
             return None
-        code = 6 if self.facets else {"": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.hex_model]
+        if self.facets:
+            code = 7 if self.facet_exp else 6
+        else:
+            code = {"": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.hex_model]
         return np.where(e != 0.0, code, 0).astype(np.int32)
 
     def mobility_models(self) -> Optional[np.ndarray]:
-        """P x P mobility model codes (0 ISO, 1 CUBIC, 3..5 HEX*)."""
+        """P x P mobility model codes (0 ISO, 1 CUBIC, 3..5 HEX*, 6 FACETED)."""
         if not self.mobility_model or self.phase_cubic_eps is None:
             return None
-        code = {"CUBIC": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5}[self.mobility_model]
+        code = {"CUBIC": 1, "HEXBOETTGER": 3, "HEXSUN": 4, "HEXYANG": 5, "FACETED": 6}[self.mobility_model]
         return np.where(np.array(self.phase_cubic_eps) != 0.0, code, 0).astype(np.int32)
 
     def mobility_eps_table(self) -> Optional[np.ndarray]:
@@ -113,13 +119,23 @@ class Case:
         em = self.energy_models()
         if not self.facets or em is None:
             return None
+        return self._facet_rows(em, (6, 7), self.facets, self.facet_families)
+
+    def mobility_facet_tables(self):
+        """(start[P*P+1], data[F, 5], family[P*P]) for the FACETED mobility pairs, or None."""
+        mm = self.mobility_models()
+        if not self.mobility_facets or mm is None:
+            return None
+        return self._facet_rows(mm, (6,), self.mobility_facets, self.mobility_facet_families)
+
+    def _facet_rows(self, codes, which, facets, families):
         P = self.nphases
         start, rows = [0], []
         for q in range(P * P):
-            if em.flat[q] == 6:
-                rows += [list(f) for f in self.facets]
+            if codes.flat[q] in which:
+                rows += [list(f) for f in facets]
             start.append(len(rows))
-        fam = np.full(P * P, int(self.facet_families), dtype=np.int32)
+        fam = np.full(P * P, int(families), dtype=np.int32)
         return np.array(start, dtype=np.int32), np.array(rows, dtype=np.float64).reshape(-1, 5), fam
 
     def model_eps(self) -> Optional[np.ndarray]:

@@ -58,8 +58,10 @@ class Context:
     # ---- parameters
     def set_model(self, sigma, mu, *, limit=None, limiting=True, regularization=1.0, tj_factor=0.0,
                   consider_nucleus_volume=True, nucleus_volume_factor=1.0, energy_model=None, cubic_eps=None,
-                  phase_solid=None, model_eps=None, facets=None, mobility_model=None, mobility_eps=None):
-        """facets: (facet_start[P*P+1], facet_data[F, 5], facet_family[P*P]) of the FACETED pairs."""
+                  phase_solid=None, model_eps=None, facets=None, mobility_model=None, mobility_eps=None,
+                  mobility_facets=None):
+        """facets: (facet_start[P*P+1], facet_data[F, 5], facet_family[P*P]) of the FACETED and
+        FACETEDEXP pairs; mobility_facets: the same for the FACETED mobility pairs."""
         sigma = np.ascontiguousarray(np.atleast_2d(sigma), dtype=np.float64)
         mu = np.ascontiguousarray(np.atleast_2d(mu), dtype=np.float64)
         lim = None if limit is None else np.ascontiguousarray(np.atleast_2d(limit), dtype=np.float64)
@@ -72,6 +74,10 @@ class Context:
         fs, fd, ff = (None, None, None) if facets is None else (
             np.ascontiguousarray(facets[0], dtype=np.int32), np.ascontiguousarray(facets[1], dtype=np.float64),
             np.ascontiguousarray(facets[2], dtype=np.int32))
+        ms, md, mf = (None, None, None) if mobility_facets is None else (
+            np.ascontiguousarray(mobility_facets[0], dtype=np.int32),
+            np.ascontiguousarray(mobility_facets[1], dtype=np.float64),
+            np.ascontiguousarray(mobility_facets[2], dtype=np.int32))
         as_ptr = lambda a, t: a.ctypes.data_as(C.POINTER(t)) if a is not None else None  # noqa: E731
         m = Model(nphases=sigma.shape[0], sigma=as_ptr(sigma, C.c_double), mu=as_ptr(mu, C.c_double),
                   limit=as_ptr(lim, C.c_double), limiting=int(limiting), regularization=regularization,
@@ -80,7 +86,9 @@ class Context:
                   cubic_eps=as_ptr(eps, C.c_double), phase_solid=as_ptr(sol, C.c_int32),
                   model_eps=as_ptr(meps, C.c_double), facet_start=as_ptr(fs, C.c_int32),
                   facet_data=as_ptr(fd, C.c_double), facet_family=as_ptr(ff, C.c_int32),
-                  mobility_model=as_ptr(mm, C.c_int32), mobility_eps=as_ptr(mme, C.c_double))
+                  mobility_model=as_ptr(mm, C.c_int32), mobility_eps=as_ptr(mme, C.c_double),
+                  mobility_facet_start=as_ptr(ms, C.c_int32), mobility_facet_data=as_ptr(md, C.c_double),
+                  mobility_facet_family=as_ptr(mf, C.c_int32))
         _check(lib().opgpu_set_model(self.h, C.byref(m)), self.h, "set_model")
 
     def set_averaging(self, enable: bool, range_: int = 0, threshold: float = 0.0):
@@ -298,7 +306,8 @@ class Context:
                       regularization=case.regularization, tj_factor=case.tj_factor,
                       energy_model=case.energy_models(), cubic_eps=case.cubic_eps(), phase_solid=case.solid_phase(),
                       model_eps=case.model_eps(), facets=case.facet_tables(),
-                      mobility_model=case.mobility_models(), mobility_eps=case.mobility_eps_table())
+                      mobility_model=case.mobility_models(), mobility_eps=case.mobility_eps_table(),
+                      mobility_facets=case.mobility_facet_tables())
         ctx.set_grains(case.ngrains, phase=case.grain_phase())
         if case.orientations:
             ctx.set_orientations(case.quaternions())

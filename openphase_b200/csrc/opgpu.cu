@@ -653,8 +653,8 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
         sp.mu_p[q] = m->mu[q];
         const double lim = m->limit ? m->limit[q] : 0.95;   // src/DrivingForce.cpp:161
         const int model = m->energy_model ? m->energy_model[q] : 0;
-        if (model < 0 || model > 6)
-            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) .. 6 (FACETED)");
+        if (model < 0 || model > 7)
+            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: energy model 0 (ISO) .. 7 (FACETEDEXP)");
         sp.emodel[q] = (signed char)model;
         const bool normal_model = model == 1 || (model >= 3 && model <= 5);
         sp.eps_p[q] = (normal_model && m->cubic_eps) ? m->cubic_eps[q] : 0.0;
@@ -691,6 +691,26 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
             sp.sigma_p[q] = energy;
             sp.maxe_p[q] = maxe;
         }
+        if (model == 7)
+        {
+            // ReadInputFacetedEXP (InterfaceEnergyModel.h:248-295): facet rows (unit normal,
+            // EpsilonEF, PowerEF); Energy = MaxEnergy = $Sigma
+            if (!m->facet_start || !m->facet_data || m->facet_start[q + 1] <= m->facet_start[q])
+                return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: a FACETEDEXP pair needs facets");
+            const bool family = m->facet_family && m->facet_family[q];
+            sp.facet_lo[q] = (int)(facet_rows.size() / 5);
+            for (int f = m->facet_start[q]; f < m->facet_start[q + 1]; f++)
+            {
+                const double* d = m->facet_data + 5 * (size_t)f;
+                if (!(d[4] >= 2.0))
+                    return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: FACETEDEXP facet power must be >= 2");
+                std::vector<double> nrm;
+                facet_normals(std::lround(d[0]), std::lround(d[1]), std::lround(d[2]), family, nrm);
+                for (size_t r = 0; r < nrm.size(); r += 3)
+                    facet_rows.insert(facet_rows.end(), {nrm[r], nrm[r + 1], nrm[r + 2], d[3], d[4]});
+            }
+            sp.facet_hi[q] = (int)(facet_rows.size() / 5);
+        }
         // src/DrivingForce.cpp:548-552: Limit*Prefactor*MaxEnergy, then *= RegularizationFactor
         double allowed = lim * sp.pref_df * sp.maxe_p[q];
         allowed *= m->regularization;
@@ -699,10 +719,33 @@ extern "C" uint32_t opgpu_set_model(opgpu_ctx* ctx, const opgpu_model* m)
     for (int q = 0; q < P * P; q++)
     {
         const int mm = m->mobility_model ? m->mobility_model[q] : 0;
-        if (mm != 0 && mm != 1 && (mm < 3 || mm > 5))
-            return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: mobility model 0 (ISO), 1 (CUBIC), 3..5 (HEX*)");
+        if (mm != 0 && mm != 1 && (mm < 3 || mm > 6))
+            return fail(ctx, OPGPU_E_INVALID,
+                        "opgpu_set_model: mobility model 0 (ISO), 1 (CUBIC), 3..5 (HEX*), 6 (FACETED)");
         sp.mmodel[q] = (signed char)mm;
         for (int k = 0; k < 4; k++) sp.meps[q][k] = (mm != 0 && m->mobility_eps) ? m->mobility_eps[4 * q + k] : 0.0;
+        sp.mfacet_lo[q] = sp.mfacet_hi[q] = 0;
+        if (mm == 6)
+        {
+            // InterfaceMobilityModel::ReadInputFaceted (InterfaceMobilityModel.h:165-208): facet
+            // rows (unit normal, MuF, EpsilonMF); it reads no $Mu, so its Mobility (the value where
+            // no solid grain of the pair counts) keeps the constructor's 0
+            const int32_t* fs = m->mobility_facet_start;
+            if (!fs || !m->mobility_facet_data || fs[q + 1] <= fs[q])
+                return fail(ctx, OPGPU_E_INVALID, "opgpu_set_model: a FACETED mobility pair needs facets");
+            const bool family = m->mobility_facet_family && m->mobility_facet_family[q];
+            sp.mfacet_lo[q] = (int)(facet_rows.size() / 5);
+            for (int f = fs[q]; f < fs[q + 1]; f++)
+            {
+                const double* d = m->mobility_facet_data + 5 * (size_t)f;
+                std::vector<double> nrm;
+                facet_normals(std::lround(d[0]), std::lround(d[1]), std::lround(d[2]), family, nrm);
+                for (size_t r = 0; r < nrm.size(); r += 3)
+                    facet_rows.insert(facet_rows.end(), {nrm[r], nrm[r + 1], nrm[r + 2], d[3], d[4]});
+            }
+            sp.mfacet_hi[q] = (int)(facet_rows.size() / 5);
+            sp.mu_p[q] = 0.0;
+        }
     }
     sp.aniso = 0;   // models of the interface normal (the disorientation energy depends on the grain pair only)
     for (int q = 0; q < P * P; q++) sp.aniso |= sp.emodel[q] == 1 || sp.emodel[q] >= 3 || sp.mmodel[q] != 0;

@@ -95,6 +95,7 @@ struct StepParams {
     double eps_x[kMaxPhases * kMaxPhases][3];
     int facet_lo[kMaxPhases * kMaxPhases], facet_hi[kMaxPhases * kMaxPhases];   // FACETED: rows of facets
     signed char mmodel[kMaxPhases * kMaxPhases];   // mobility model per phase pair (codes of emodel)
+    int mfacet_lo[kMaxPhases * kMaxPhases], mfacet_hi[kMaxPhases * kMaxPhases];   // FACETED mobility rows
     double meps[kMaxPhases * kMaxPhases][4];       // its Epsilon1..4
     double maxe_p[kMaxPhases * kMaxPhases];
     signed char solid_p[kMaxPhases];

@@ -156,8 +156,8 @@ __device__ __forceinline__ void interface_orientation(const double* g3, const do
 
 // InterfaceEnergyModel::Calculate (include/InterfaceProperties/InterfaceEnergyModel.h:325-399) for
 // the models of the interface normal n: CUBIC, HEXBOETTGER (Boettger et al. 2006), HEXSUN (Sun et
-// al. 2006), HEXYANG (Yang et al. 2015) and FACETED (facet rows: unit normal, SigmaF, EpsilonEF),
-// in the reference's operation order.
+// al. 2006), HEXYANG (Yang et al. 2015), FACETED (facet rows: unit normal, SigmaF, EpsilonEF) and
+// FACETEDEXP (rows: unit normal, EpsilonEF, PowerEF), in the reference's operation order.
 __device__ __forceinline__ double model_energy(const StepParams& p, int q, const double* n, const double* facets)
 {
     const double E = p.sigma_p[q], e1 = p.eps_p[q];
@@ -198,20 +198,51 @@ __device__ __forceinline__ double model_energy(const StepParams& p, int q, const
             const double sin2 = 1.0 - cos2;
             return ea * epa * epa * pow(sqrt(sin2 + epa * epa * cos2), -3.0);
         }
+        case 7:
+        {
+            // FACETEDEXP (InterfaceEnergyModel.h:389-413): every facet facing the normal lowers the
+            // energy by E*eps*cos^p and adds its second-order term E*eps*p*cos^p (rows: unit
+            // normal, EpsilonEF, PowerEF)
+            double loc = E;
+            for (int f = p.facet_lo[q]; f < p.facet_hi[q]; f++)
+            {
+                const double* r = facets + 5 * f;
+                const double c = x * r[0] + y * r[1] + z * r[2];
+                if (c > 0.0)
+                {
+                    loc -= E * r[3] * pow(c, r[4]);
+                    loc += E * r[3] * r[4] * pow(c, r[4]);
+                }
+            }
+            return loc;
+        }
         default:
             return E * (1.0 + e1 * (1.5 - 2.5 * (pow(x, 4.0) + pow(y, 4.0) + pow(z, 4.0))));
     }
 }
 
 // InterfaceMobilityModel::Calculate (include/InterfaceProperties/InterfaceMobilityModel.h:210-265):
-// CUBIC, HEXBOETTGER, HEXSUN, HEXYANG of the interface normal n, in the reference's operation order
+// CUBIC, HEXBOETTGER, HEXSUN, HEXYANG and FACETED of the interface normal n, in the reference's operation order
 // (the signs of the anisotropy terms differ from the energy models').
-__device__ __forceinline__ double mobility_model(const StepParams& p, int q, const double* n)
+__device__ __forceinline__ double mobility_model(const StepParams& p, int q, const double* n, const double* facets)
 {
     const double M = p.mu_p[q], e1 = p.meps[q][0], e2 = p.meps[q][1], e3 = p.meps[q][2], e4 = p.meps[q][3];
     const double x = n[0], y = n[1], z = n[2];
     switch (p.mmodel[q])
     {
+        case 6:
+        {
+            // FACETED (InterfaceMobilityModel.h:266-288): the facet of smallest inclination
+            // acos(n.f) (the last one on ties) sets MuF*(EpsMF + (1 - EpsMF)|tan i| tanh(1/|tan i|))
+            double incl = 3.14159265358979323846, ma = 0.0, ea = 0.0;
+            for (int f = p.mfacet_lo[q]; f < p.mfacet_hi[q]; f++)
+            {
+                const double* r = facets + 5 * f;
+                const double d = acos(x * r[0] + y * r[1] + z * r[2]);
+                if (fabs(d) <= fabs(incl)) { incl = d; ma = r[3]; ea = r[4]; }
+            }
+            return ma * (ea + (1.0 - ea) * fabs(tan(incl)) * tanh(pow(fabs(tan(incl)), -1.0)));
+        }
         case 3:
             return M * (1.0 + e1 * (pow(x, 6.0) - pow(y, 6.0) - 15.0 * pow(x, 4.0) * y * y + 15.0 * pow(y, 4.0) * x * x
                                     + (5.0 * pow(z, 4.0) - 5.0 * pow(z, 2.0) + pow(z, 6.0))));
@@ -256,7 +287,7 @@ __device__ __forceinline__ double voxel_mobility(const StepParams& p, const Step
         const double g3[3] = {(double)sc.grad[(3 * e) * S], (double)sc.grad[(3 * e + 1) * S], (double)sc.grad[(3 * e + 2) * S]};
         double n[3];
         interface_orientation(g3, a.grot + 9 * (long long)g, n);
-        loc += mobility_model(p, q, n);
+        loc += mobility_model(p, q, n, a.facets);
         solids++;
     }
     if (solids == 0) loc = p.mu_p[q];

@@ -31,7 +31,8 @@ class OpParams(C.Structure):
                 ("mu_phase", C.c_void_p), ("energy_model", C.c_void_p), ("cubic_eps", C.c_void_p),
                 ("model_eps", C.c_void_p), ("facet_start", C.c_void_p), ("facet_data", C.c_void_p),
                 ("facet_family", C.c_void_p), ("mobility_model", C.c_void_p), ("mobility_eps", C.c_void_p),
-                ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
+                ("mobility_facet_start", C.c_void_p), ("mobility_facet_data", C.c_void_p),
+                ("mobility_facet_family", C.c_void_p), ("quat", C.c_void_p), ("pair_sigma", C.c_void_p), ("pair_mu", C.c_void_p), ("dg", C.c_void_p),
                 ("limiting", C.c_int), ("limit_phase", C.c_void_p), ("regularization", C.c_double),
                 ("tj_factor", C.c_double), ("consider_nucleus_volume", C.c_int),
                 ("nucleus_volume_factor", C.c_double), ("threads", C.c_int), ("average", C.c_int)]
@@ -113,6 +114,8 @@ class Oracle:
         mm = keep(mm) if mm is not None else None
         mme = case.mobility_eps_table()
         mme = keep(mme) if mme is not None else None
+        mfac = case.mobility_facet_tables()
+        mfac = tuple(keep(x) for x in mfac) if mfac is not None else None
         quat = case.quaternions()
         quat = keep(quat.astype(np.float64)) if quat is not None else None
         ps = case.pair_sigma()
@@ -130,6 +133,9 @@ class Oracle:
                      facet_family=_p(fac[2]).value if fac else None,
                      mobility_model=_p(mm).value if mm is not None else None,
                      mobility_eps=_p(mme).value if mme is not None else None,
+                     mobility_facet_start=_p(mfac[0]).value if mfac else None,
+                     mobility_facet_data=_p(mfac[1]).value if mfac else None,
+                     mobility_facet_family=_p(mfac[2]).value if mfac else None,
                      quat=_p(quat).value if quat is not None else None, pair_sigma=_p(ps).value if ps is not None else None, pair_mu=None,
                      dg=_p(dg).value if dg is not None else None, limiting=int(case.limiting),
                      limit_phase=_p(lim).value, regularization=case.regularization, tj_factor=case.tj_factor,
@@ -240,7 +246,7 @@ def _case_text(case, workdir: Path, dump_steps, threads, nsteps=None, vtk_steps=
             if case.disorientation:
                 lines.append(f"energy_model {a} {b} DISORIENTATION")
             elif case.facets and eps is not None and eps[a, b] != 0.0:
-                lines.append(f"energy_model {a} {b} FACETED")
+                lines.append(f"energy_model {a} {b} {'FACETEDEXP' if case.facet_exp else 'FACETED'}")
                 lines.append(f"facet_family {a} {b} {int(case.facet_families)}")
                 for (h, k, l, sf, ef) in case.facets:
                     lines.append(f"facet {a} {b} {h} {k} {l} {float(sf)!r} {float(ef)!r}")
@@ -256,6 +262,10 @@ def _case_text(case, workdir: Path, dump_steps, threads, nsteps=None, vtk_steps=
                 if mm[a, b]:
                     lines.append(f"mobility_model {a} {b} {case.mobility_model}")
                     lines.append(f"mobility_eps {a} {b} " + " ".join(repr(float(e)) for e in case.mobility_eps))
+                    if case.mobility_model == "FACETED":
+                        lines.append(f"mobility_facet_family {a} {b} {int(case.mobility_facet_families)}")
+                        for (h, k, l, mf, ef) in case.mobility_facets:
+                            lines.append(f"mobility_facet {a} {b} {h} {k} {l} {float(mf)!r} {float(ef)!r}")
     if P > 1:
         f = workdir / "grain_phase.bin"
         case.grain_phase().astype(np.int32).tofile(f)

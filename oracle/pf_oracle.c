@@ -37,6 +37,7 @@ struct op_sim {
     double* model_eps;            /* [P*P*3] Epsilon2..4                                         */
     double* facets;               /* FACETED rows: unit facet normal (3), SigmaF, EpsilonEF      */
     int* facet_lo; int* facet_hi; /* [P*P] rows of each pair                                     */
+    int* mfacet_lo; int* mfacet_hi;   /* [P*P] FACETED mobility rows (unit normal, MuF, EpsilonMF) */
     double* phase_e; double* phase_maxe;   /* [P*P] FACETED Energy (mean SigmaF), MaxEnergy      */
     int* mobility_model;          /* [P*P]                                                       */
     double* mobility_eps;         /* [P*P*4]                                                     */
@@ -84,6 +85,31 @@ static int facet_family_vectors(long h, long k, long l, int family, long w[48][3
     return n;
 }
 static double dmin(double a, double b) { return (b < a) ? b : a; }   /* std::min */
+
+/* Append the normalised facet vectors of facet row d (h, k, l, c1, c2) to the row table, each with
+ * the row's two values; iVector3::normalized (include/Containers/iVector3.h:274-289). */
+static void append_facet(double** rows_p, int* rows, int* cap_rows, const double* d, int family)
+{
+    long w[48][3];
+    const int nw = facet_family_vectors(lround(d[0]), lround(d[1]), lround(d[2]), family, w);
+    if (*rows + nw > *cap_rows)
+    {
+        *cap_rows = 2*(*rows + nw);
+        *rows_p = (double*)realloc(*rows_p, (size_t)(*cap_rows)*5*sizeof(double));
+    }
+    for (int k = 0; k < nw; k++)
+    {
+        double* r = *rows_p + 5*(size_t)(*rows)++;
+        const double norm = sqrt((double)(w[k][0]*w[k][0] + w[k][1]*w[k][1] + w[k][2]*w[k][2]));
+        if (norm != 0.0)
+        {
+            const double inv = 1.0/norm;
+            r[0] = w[k][0]*inv; r[1] = w[k][1]*inv; r[2] = w[k][2]*inv;
+        }
+        else { r[0] = 0.0; r[1] = 0.0; r[2] = 0.0; }
+        r[3] = d[3]; r[4] = d[4];
+    }
+}
 
 static double* dup_d(const double* src, size_t n)
 {
@@ -188,9 +214,13 @@ op_sim* op_create(const op_params* p, int cap)
     }
     if (p->model_eps) memcpy(s->model_eps, p->model_eps, (size_t)P*P*3*sizeof(double));
     /* ReadInputFaceted (InterfaceEnergyModel.h:196-246): facet normals (families expanded), Energy
-     * = mean SigmaF accumulated in facet order, MaxEnergy = max SigmaF */
+     * = mean SigmaF accumulated in facet order, MaxEnergy = max SigmaF.  ReadInputFacetedEXP
+     * (:248-295): the same rows with EpsilonEF and PowerEF; Energy = MaxEnergy = $Sigma.  The
+     * FACETED mobility (InterfaceMobilityModel.h:165-208): rows with MuF and EpsilonMF. */
     s->facet_lo = (int*)calloc((size_t)P*P, sizeof(int));
     s->facet_hi = (int*)calloc((size_t)P*P, sizeof(int));
+    s->mfacet_lo = (int*)calloc((size_t)P*P, sizeof(int));
+    s->mfacet_hi = (int*)calloc((size_t)P*P, sizeof(int));
     s->phase_e = (double*)calloc((size_t)P*P, sizeof(double));
     s->phase_maxe = (double*)calloc((size_t)P*P, sizeof(double));
     s->facets = NULL;
@@ -198,7 +228,8 @@ op_sim* op_create(const op_params* p, int cap)
         int rows = 0, cap_rows = 0;
         for (int q = 0; q < P*P; q++)
         {
-            if (!p->energy_model || p->energy_model[q] != OP_ENERGY_FACETED || !p->facet_start) continue;
+            const int em = p->energy_model ? p->energy_model[q] : 0;
+            if ((em != OP_ENERGY_FACETED && em != OP_ENERGY_FACETEDEXP) || !p->facet_start) continue;
             const int n0 = p->facet_start[q], n1 = p->facet_start[q + 1], nf = n1 - n0;
             const int family = p->facet_family ? p->facet_family[q] : 0;
             double energy = 0.0, maxe = 0.0;
@@ -206,32 +237,22 @@ op_sim* op_create(const op_params* p, int cap)
             for (int f = n0; f < n1; f++)
             {
                 const double* d = p->facet_data + 5*(size_t)f;
-                long w[48][3];
-                const int nw = facet_family_vectors(lround(d[0]), lround(d[1]), lround(d[2]), family, w);
-                if (rows + nw > cap_rows)
-                {
-                    cap_rows = 2*(rows + nw);
-                    s->facets = (double*)realloc(s->facets, (size_t)cap_rows*5*sizeof(double));
-                }
-                for (int k = 0; k < nw; k++)
-                {
-                    double* r = s->facets + 5*(size_t)rows++;
-                    /* iVector3::normalized (include/Containers/iVector3.h:274-289) */
-                    const double norm = sqrt((double)(w[k][0]*w[k][0] + w[k][1]*w[k][1] + w[k][2]*w[k][2]));
-                    if (norm != 0.0)
-                    {
-                        const double inv = 1.0/norm;
-                        r[0] = w[k][0]*inv; r[1] = w[k][1]*inv; r[2] = w[k][2]*inv;
-                    }
-                    else { r[0] = 0.0; r[1] = 0.0; r[2] = 0.0; }
-                    r[3] = d[3]; r[4] = d[4];
-                }
+                append_facet(&s->facets, &rows, &cap_rows, d, family);
                 energy += d[3]/nf;
                 if (d[3] > maxe) maxe = d[3];
             }
             s->facet_hi[q] = rows;
-            s->phase_e[q] = energy;
-            s->phase_maxe[q] = maxe;
+            if (em == OP_ENERGY_FACETED) { s->phase_e[q] = energy; s->phase_maxe[q] = maxe; }
+        }
+        for (int q = 0; q < P*P; q++)
+        {
+            const int mm = p->mobility_model ? p->mobility_model[q] : 0;
+            if (mm != OP_MOBILITY_FACETED || !p->mobility_facet_start) continue;
+            const int family = p->mobility_facet_family ? p->mobility_facet_family[q] : 0;
+            s->mfacet_lo[q] = rows;
+            for (int f = p->mobility_facet_start[q]; f < p->mobility_facet_start[q + 1]; f++)
+                append_facet(&s->facets, &rows, &cap_rows, p->mobility_facet_data + 5*(size_t)f, family);
+            s->mfacet_hi[q] = rows;
         }
     }
     s->aniso = 0;
@@ -317,6 +338,7 @@ void op_destroy(op_sim* s)
     free(s->pair_sigma); free(s->pair_mu); free(s->dg);
     free(s->energy_model); free(s->cubic_eps); free(s->model_eps); free(s->rot); free(s->quat);
     free(s->facets); free(s->facet_lo); free(s->facet_hi); free(s->phase_e); free(s->phase_maxe);
+    free(s->mfacet_lo); free(s->mfacet_hi);
     free(s->mobility_model); free(s->mobility_eps);
     free(s->cnt); free(s->cnt2); free(s->e); free(s->e2); free(s->flag);
     free(s->volume); free(s->max_volume); free(s->ref_volume); free(s->vr);
@@ -497,6 +519,23 @@ static double model_energy(const op_sim* s, int q, const double n[3])
             const double sin2 = 1.0 - cos2;
             return ea*epa*epa*pow(sqrt(sin2 + epa*epa*cos2), -3.0);
         }
+        case OP_ENERGY_FACETEDEXP:
+        {
+            /* InterfaceEnergyModel::Calculate, FacetedEXP (:389-413): every facet with cos > 0
+             * subtracts E*eps*cos^p and adds E*eps*p*cos^p */
+            double loc = E;
+            for (int f = s->facet_lo[q]; f < s->facet_hi[q]; f++)
+            {
+                const double* r = s->facets + 5*f;
+                const double c = x*r[0] + y*r[1] + z*r[2];
+                if (c > 0.0)
+                {
+                    loc -= E*r[3]*pow(c, r[4]);
+                    loc += E*r[3]*r[4]*pow(c, r[4]);
+                }
+            }
+            return loc;
+        }
         case OP_ENERGY_HEXYANG:
             return E*(1.0 + e1*pow((3.0*z*z - 1.0), 2) + ex[0]*pow((x*x*x - 3.0*x*y*y), 2)*pow((9.0*z*z - 1.0 + ex[1]), 2));
         default:   /* CUBIC */
@@ -553,6 +592,19 @@ static double mobility_model(const op_sim* s, int q, const double n[3])
     const double x = n[0], y = n[1], z = n[2];
     switch (s->mobility_model[q])
     {
+        case OP_MOBILITY_FACETED:
+        {
+            /* InterfaceMobilityModel::Calculate, Faceted (:266-288): the facet of smallest
+             * inclination acos(n.f), the last one on ties */
+            double incl = OP_PI, ma = 0.0, ea = 0.0;
+            for (int f = s->mfacet_lo[q]; f < s->mfacet_hi[q]; f++)
+            {
+                const double* r = s->facets + 5*f;
+                const double d = acos(x*r[0] + y*r[1] + z*r[2]);
+                if (fabs(d) <= fabs(incl)) { incl = d; ma = r[3]; ea = r[4]; }
+            }
+            return ma*(ea + (1.0 - ea)*fabs(tan(incl))*tanh(pow(fabs(tan(incl)), -1.0)));
+        }
         case OP_ENERGY_HEXBOETTGER:
             return M*(1.0 + e[0]*(pow(x, 6) - pow(y, 6) - 15.0*pow(x, 4)*y*y + 15.0*pow(y, 4)*x*x
                                   + (5.0*pow(z, 4) - 5.0*pow(z, 2) + pow(z, 6))));
@@ -593,7 +645,9 @@ static double voxel_mobility(const op_sim* s, const entry* L, int a, int b)
         loc += mobility_model(s, q, n);
         solids++;
     }
-    if (solids == 0) loc = s->mu_phase[q];
+    /* Mobility: $Mu, except the FACETED model, which reads none and keeps the constructor's 0
+     * (InterfaceMobilityModel.h:51-56, 165-208) */
+    if (solids == 0) loc = s->mobility_model[q] == OP_MOBILITY_FACETED ? 0.0 : s->mu_phase[q];
     return loc;
 }
 

@@ -20,7 +20,8 @@ extern "C" {
 enum { OP_STENCIL_SIMPLE = 0, OP_STENCIL_ISOTROPIC = 1, OP_STENCIL_LB = 2 };
 enum { OP_STAGE_STABLE = 0, OP_STAGE_SEED = 1, OP_STAGE_NUCLEUS = 2 };
 enum { OP_ENERGY_ISO = 0, OP_ENERGY_CUBIC = 1, OP_ENERGY_DISORIENTATION = 2, OP_ENERGY_HEXBOETTGER = 3,
-       OP_ENERGY_HEXSUN = 4, OP_ENERGY_HEXYANG = 5, OP_ENERGY_FACETED = 6 };
+       OP_ENERGY_HEXSUN = 4, OP_ENERGY_HEXYANG = 5, OP_ENERGY_FACETED = 6, OP_ENERGY_FACETEDEXP = 7 };
+enum { OP_MOBILITY_FACETED = 6 };   /* mobility models use the energy codes 0, 1, 3..5, and this */
 
 /* Status bits reported by op_step (OR-ed over all voxels and steps since the last call). */
 enum {
@@ -46,10 +47,14 @@ typedef struct op_params {
     const double* cubic_eps;          /* [P*P] Epsilon1 of the CUBIC / HEX models (NULL: 0)     */
     const double* model_eps;          /* [P*P*3] Epsilon2..4 of the HEX models (NULL: 0)        */
     const int* facet_start;           /* [P*P+1] FACETED: facets of pair q in facet_data rows    */
-    const double* facet_data;         /* rows of h, k, l, SigmaF, EpsilonEF                       */
+    const double* facet_data;         /* rows of h, k, l, SigmaF, EpsilonEF (FACETEDEXP: h, k, l,
+                                         EpsilonEF, PowerEF)                                       */
     const int* facet_family;          /* [P*P] 1: facets stand for their families                */
     const int* mobility_model;        /* [P*P] 0 ISO, 1 CUBIC, 3..5 HEX* (NULL: all ISO)         */
     const double* mobility_eps;       /* [P*P*4] its Epsilon1..4                                  */
+    const int* mobility_facet_start;  /* [P*P+1] FACETED mobility: facets of pair q               */
+    const double* mobility_facet_data;/* rows of h, k, l, MuF, EpsilonMF                          */
+    const int* mobility_facet_family; /* [P*P] 1: facets stand for their families                */
     const double* quat;               /* [G*4] grain orientation quaternions (w,x,y,z) or NULL  */
     const double* pair_sigma;         /* [G*G] per-grain-pair sigma overriding the phase value, or NULL */
     const double* pair_mu;            /* [G*G] per-grain-pair mobility, or NULL                 */

@@ -65,6 +65,8 @@ struct Case
     std::map<std::pair<int,int>, std::vector<double>> model_eps;   // Epsilon2..4 of the HEX models
     std::map<std::pair<int,int>, std::vector<std::vector<double>>> facets;   // FACETED: h k l SigmaF EpsilonEF
     std::map<std::pair<int,int>, int> facet_family;
+    std::map<std::pair<int,int>, std::vector<std::vector<double>>> mobility_facets;   // FACETED mobility: h k l MuF EpsilonMF
+    std::map<std::pair<int,int>, int> mobility_facet_family;
     std::map<std::pair<int,int>, std::string> mobility_model;
     std::map<std::pair<int,int>, std::vector<double>> mobility_eps;
     std::map<std::pair<int,int>, std::string> energy_model;
@@ -135,6 +137,8 @@ static Case parse_case(const std::string& path)
         else if (key == "mobility_eps") { int a, b; std::vector<double> e(4); is >> a >> b >> e[0] >> e[1] >> e[2] >> e[3]; c.mobility_eps[{a,b}] = e; }
         else if (key == "facet_family") { int a, b, f; is >> a >> b >> f; c.facet_family[{a,b}] = f; }
         else if (key == "facet") { int a, b; std::vector<double> f(5); is >> a >> b >> f[0] >> f[1] >> f[2] >> f[3] >> f[4]; c.facets[{a,b}].push_back(f); }
+        else if (key == "mobility_facet_family") { int a, b, f; is >> a >> b >> f; c.mobility_facet_family[{a,b}] = f; }
+        else if (key == "mobility_facet") { int a, b; std::vector<double> f(5); is >> a >> b >> f[0] >> f[1] >> f[2] >> f[3] >> f[4]; c.mobility_facets[{a,b}].push_back(f); }
         else if (key == "model_eps") { int a, b; double e2, e3, e4; is >> a >> b >> e2 >> e3 >> e4; c.model_eps[{a,b}] = {e2, e3, e4}; }
         else if (key == "ngrains") is >> c.ngrains;
         else if (key == "grain_phase_file") is >> grain_phase_file;
@@ -199,15 +203,21 @@ static void write_opi(const Case& c, const std::string& path)
         if (model == "HEXSUN")
             o << "$EpsilonE20_" << ab << " : " << e1 << "\n" << "$EpsilonE40_" << ab << " : " << ex[0] << "\n"
               << "$EpsilonE60_" << ab << " : " << ex[1] << "\n" << "$EpsilonE66_" << ab << " : " << ex[2] << "\n";
-        if (model == "FACETED")
+        if (model == "FACETED" or model == "FACETEDEXP")
         {
             const auto& fs = c.facets.at({a,b});
             const bool fam = c.facet_family.count({a,b}) and c.facet_family.at({a,b});
             o << (fam ? "$NfacetFamilies_" : "$Nfacets_") << ab << " : " << fs.size() << "\n";
             for (size_t n = 0; n < fs.size(); n++)
-                o << "$Facet_" << ab << "_" << n << " : " << (long)fs[n][0] << " " << (long)fs[n][1] << " " << (long)fs[n][2] << "\n"
-                  << "$SigmaF_" << ab << "_" << n << " : " << fs[n][3] << "\n"
-                  << "$EpsilonEF_" << ab << "_" << n << " : " << fs[n][4] << "\n";
+            {
+                o << "$Facet_" << ab << "_" << n << " : " << (long)fs[n][0] << " " << (long)fs[n][1] << " " << (long)fs[n][2] << "\n";
+                if (model == "FACETED")
+                    o << "$SigmaF_" << ab << "_" << n << " : " << fs[n][3] << "\n"
+                      << "$EpsilonEF_" << ab << "_" << n << " : " << fs[n][4] << "\n";
+                else
+                    o << "$EpsilonEF_" << ab << "_" << n << " : " << fs[n][3] << "\n"
+                      << "$PowerEF_" << ab << "_" << n << " : " << fs[n][4] << "\n";
+            }
         }
         if (model == "HEXYANG")
             o << "$EpsilonE1_" << ab << " : " << e1 << "\n" << "$EpsilonE2_" << ab << " : " << ex[0] << "\n"
@@ -222,6 +232,18 @@ static void write_opi(const Case& c, const std::string& path)
         if (mmodel == "HEXYANG")
             o << "$EpsilonM1_" << ab << " : " << me[0] << "\n" << "$EpsilonM2_" << ab << " : " << me[1] << "\n"
               << "$EpsilonM3_" << ab << " : " << me[2] << "\n";
+        if (mmodel == "FACETED")
+        {
+            // the energy and mobility models read the same $NfacetFamilies / $Facet keys: a pair
+            // with both FACETED shares its facet vectors (not used here)
+            const auto& fs = c.mobility_facets.at({a,b});
+            const bool fam = c.mobility_facet_family.count({a,b}) and c.mobility_facet_family.at({a,b});
+            o << (fam ? "$NfacetFamilies_" : "$Nfacets_") << ab << " : " << fs.size() << "\n";
+            for (size_t n = 0; n < fs.size(); n++)
+                o << "$Facet_" << ab << "_" << n << " : " << (long)fs[n][0] << " " << (long)fs[n][1] << " " << (long)fs[n][2] << "\n"
+                  << "$MuF_" << ab << "_" << n << " : " << fs[n][3] << "\n"
+                  << "$EpsilonMF_" << ab << "_" << n << " : " << fs[n][4] << "\n";
+        }
         o << "$Mu_" << a << "_" << b << " : " << m << "\n";
     }
     o << "$TripleJunctionModel : MODEL\n";

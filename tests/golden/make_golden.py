@@ -87,6 +87,20 @@ GOLDEN_CASES = {
                                phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
                                facets=((1, 0, 0, 1.0, 0.7), (1, 1, 1, 1.1, 0.8)), name="faceted_nuclei_24"),
                           [1, 10, 30]),
+    # FACETEDEXP energy model ({100} and {111} families, cusp powers 4 and 6) on the solid-liquid pairs
+    "facetedexp_nuclei_24": (Case(24, 24, 24, 7, seed=12, iwidth=5.0, dt=0.05, sigma=1.2,
+                                  phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                                  phase_solid=(0, 1), phase_cubic_eps=((0.0, 1.0), (1.0, 0.0)),
+                                  phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                                  facets=((1, 0, 0, 0.05, 4.0), (1, 1, 1, 0.03, 6.0)), facet_exp=True,
+                                  name="facetedexp_nuclei_24"), [1, 10, 30]),
+    # FACETED mobility ({100} and {111} families) with the CUBIC energy on the solid-liquid pairs
+    "mobility_faceted_24": (Case(24, 24, 24, 7, seed=13, iwidth=5.0, dt=0.05, sigma=1.2,
+                                 phase_sigma=((1.0, 1.0), (1.0, 1.2)), phase_mu=((2.0, 2.0), (2.0, 0.5)),
+                                 phase_solid=(0, 1), phase_cubic_eps=((0.0, 0.02), (0.02, 0.0)),
+                                 phase_dg=(0.1, 0.0), init="nuclei", nucleus_radius=4.0, orientations=True,
+                                 mobility_model="FACETED", mobility_facets=((1, 0, 0, 2.0, 0.3), (1, 1, 1, 1.5, 0.5)),
+                                 name="mobility_faceted_24"), [1, 30]),
     # DISORIENTATION energy model: per-grain-pair energies from the cubic disorientation of
     # orientations spread over up to 0.6 rad (pairs below and above the 0.349 rad cap)
     "disorientation_20": (Case(20, 20, 20, 12, seed=11, iwidth=4.0, dt=0.1, orientations=True,

@@ -49,12 +49,13 @@ def test_fp64_cubic_nuclei_match_oracle(n, grains, checkpoints):
 
 
 @pytest.mark.parametrize("name", ["cubic_nuclei_24", "hexboettger_nuclei_24", "hexsun_nuclei_24",
-                                  "hexyang_nuclei_24", "faceted_nuclei_24", "mobility_cubic_24",
-                                  "mobility_hexboettger_24", "mobility_hexsun_24", "mobility_hexyang_24"])
+                                  "hexyang_nuclei_24", "faceted_nuclei_24", "facetedexp_nuclei_24",
+                                  "mobility_cubic_24", "mobility_hexboettger_24", "mobility_hexsun_24",
+                                  "mobility_hexyang_24", "mobility_faceted_24"])
 def test_fp64_energy_models_match_oracle_and_reference(name):
-    """CUBIC, the hexagonal models (HEXBOETTGER, HEXSUN, HEXYANG) and FACETED with {100} and {111}
-    facet families (InterfaceEnergyModel.h:325-438), and the anisotropic mobilities
-    (InterfaceMobilityModel.h:210-265), on the solid-liquid pairs: the FP64 form against the oracle over 100 steps and against the
+    """CUBIC, the hexagonal models (HEXBOETTGER, HEXSUN, HEXYANG), FACETED and FACETEDEXP with {100}
+    and {111} facet families (InterfaceEnergyModel.h:325-438), and the anisotropic mobilities
+    including FACETED (InterfaceMobilityModel.h:210-288), on the solid-liquid pairs: the FP64 form against the oracle over 100 steps and against the
     reference's own states (tests/golden/<name>.npz) at its checkpoints."""
     from tests.golden.make_golden import GOLDEN_CASES
     from pathlib import Path
