@@ -163,37 +163,52 @@ __device__ __forceinline__ void prefetch_counts(const StepParams& p, const StepA
     }
 }
 
-// Bring plane xp (window position wpos) into ring slot `rs`: slot lists, bitmask words and dense
-// per-slot values.  Grains not yet in the window get a slot that no grain of the window uses.
-// cr holds the plane's counts on entry (prefetched) and the next plane's counts on return.
+// Registers a thread keeps between the passes of the plane loader: the voxel index of each of its
+// records and their first kKeep entries.
+template <class R, int TY>
+struct PlaneLoad {
+    long long vv[PlaneRegs<TY>::kPer];
+    int gr[PlaneRegs<TY>::kPer][PlaneRegs<TY>::kKeep];
+    R vr[PlaneRegs<TY>::kPer][PlaneRegs<TY>::kKeep];
+};
+
+// Bringing plane xp (window position wpos) into ring slot `rs` -- slot lists, bitmask words and
+// dense per-slot values; grains not yet in the window get a slot that no grain of the window uses --
+// takes three passes with a barrier between each:
+//   plane_scan    reads the records once (the first kKeep entries stay in registers), marks the
+//                 grains already slotted as in use and collects the others in `pending`; it touches
+//                 only the hash (read), lastpos, pslot and pending, so it may run while other
+//                 threads still read the ring for the previous plane; returns whether this thread
+//                 added a pending grain
+//   plane_assign  warp 0 hands free slots to the pending grains (only needed when some thread
+//                 added one)
+//   plane_fill    slot lists, bitmask words and dense values of the incoming plane, clearing what
+//                 the ring position held before
+// cr holds the plane's counts on entry (prefetched) and the next plane's counts after plane_fill.
 // Invariant of the dense planes: dense[k][rs][r] != 0 only if bit k of word[rs][r] is set.
 template <class R, int KS, int TY>
-__device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
-                                           int rs, int xp, int wpos, int y0, int z0, int t,
-                                           int (&cr)[PlaneRegs<TY>::kPer])
+__device__ __forceinline__ bool plane_scan(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
+                                           int xp, int wpos, int y0, int z0, int t,
+                                           const int (&cr)[PlaneRegs<TY>::kPer], PlaneLoad<R, TY>& L)
 {
     using Geo = TileGeom<TY>;
     using PR = PlaneRegs<TY>;
     const long long N = p.n;
     const long long base = (long long)xp * p.ny * p.nz;
     const R* __restrict__ vin = static_cast<const R*>(a.val_in);
-    long long vv[PR::kPer];
-    int gr[PR::kPer][PR::kKeep];
-    R vr[PR::kPer][PR::kKeep];
-    // 1. read the records once (the first kKeep entries stay in registers); mark the grains already
-    //    slotted as in use, collect the others in `pending`
+    bool added = false;
 #pragma unroll
     for (int i = 0; i < PR::kPer; i++)
     {
         const int r = t + i * Geo::NT;
-        vv[i] = r < Geo::kRecs ? plane_voxel<TY>(p, base, r, y0, z0) : 0;
+        L.vv[i] = r < Geo::kRecs ? plane_voxel<TY>(p, base, r, y0, z0) : 0;
 #pragma unroll
         for (int s = 0; s < PR::kKeep; s++)
         {
             if (s < cr[i])
             {
-                gr[i][s] = a.idx_in[s * N + vv[i]];
-                vr[i][s] = vin[s * N + vv[i]];
+                L.gr[i][s] = a.idx_in[s * N + L.vv[i]];
+                L.vr[i][s] = vin[s * N + L.vv[i]];
             }
         }
     }
@@ -205,17 +220,18 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
             int g;
 #pragma unroll
             for (int q = 0; q < PR::kKeep; q++)
-                if (q == s) g = gr[i][q];
-            if (s >= PR::kKeep) g = a.idx_in[s * N + vv[i]];
+                if (q == s) g = L.gr[i][q];
+            if (s >= PR::kKeep) g = a.idx_in[s * N + L.vv[i]];
             const int k0 = find_slot(S.hkey, S.hslot, g);
             if constexpr (LoaderSlotCache<R>::value)
                 if (s < PR::kKeep) S.pslot[t + i * Geo::NT][s] = (uint8_t)(k0 >= 0 ? k0 : 0xFF);
             if (k0 >= 0)
             {
-                S.lastpos[k0] = wpos;   // in use by the incoming plane: not free for step 2
+                S.lastpos[k0] = wpos;   // in use by the incoming plane: not free for plane_assign
             }
             else
             {
+                added = true;
                 unsigned h = ((unsigned)g * 2654435761u) & 31u;
                 for (int probe = 0; probe < 32; probe++)
                 {
@@ -226,9 +242,14 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
             }
         }
     }
-    __syncthreads();
-    // 2. warp 0 hands free slots (grain gone from the window) to the pending grains; lane 0 keeps
-    //    the grain -> slot hash in step
+    return added;
+}
+
+template <class R, int KS, int TY>
+__device__ __forceinline__ void plane_assign(TileSmem<R, KS, TY>& S, int wpos, int t)
+{
+    // warp 0 hands free slots (grain gone from the window) to the pending grains; lane 0 keeps
+    // the grain -> slot hash in step
     if (t < 32)
     {
         const int g = S.pending[t];
@@ -240,7 +261,6 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
         const int rank = __popc(vm & ((1u << t) - 1u));
         const int k = (valid && rank < __popc(fm)) ? (int)__fns(fm, 0, rank + 1) : -1;
         if (valid) S.pending[t] = -1;
-        const unsigned fb = __ballot_sync(0xffffffffu, valid && k < 0);
         for (unsigned m = vm; m; m &= m - 1u)
         {
             const int lane = __ffs(m) - 1;
@@ -255,21 +275,26 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
                 S.lastpos[kl] = wpos;
             }
         }
-        if (t == 0)
+        // grains left without a slot are marked per record in plane_fill
+        if (t == 0 && S.tomb > 24)
         {
-            (void)fb;   // grains left without a slot are marked per record in step 3
-            if (S.tomb > 24)
-            {
-                for (int h = 0; h < kSlotHash; h++) S.hkey[h] = -1;
-                for (int q = 0; q < kSlots; q++)
-                    if (S.grain_of[q] >= 0) hash_insert(S.hkey, S.hslot, S.grain_of[q], q);
-                S.tomb = 0;
-            }
+            for (int h = 0; h < kSlotHash; h++) S.hkey[h] = -1;
+            for (int q = 0; q < kSlots; q++)
+                if (S.grain_of[q] >= 0) hash_insert(S.hkey, S.hslot, S.grain_of[q], q);
+            S.tomb = 0;
         }
     }
-    __syncthreads();
-    // 3. slot lists, bitmask words, dense values of the incoming plane (clearing what the ring
-    //    position held before)
+}
+
+template <class R, int KS, int TY>
+__device__ __forceinline__ void plane_fill(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
+                                           int rs, int xp, int y0, int z0, int t, int (&cr)[PlaneRegs<TY>::kPer],
+                                           const PlaneLoad<R, TY>& L)
+{
+    using Geo = TileGeom<TY>;
+    using PR = PlaneRegs<TY>;
+    const long long N = p.n;
+    const R* __restrict__ vin = static_cast<const R*>(a.val_in);
 #pragma unroll
     for (int i = 0; i < PR::kPer; i++)
     {
@@ -286,9 +311,9 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
             R val;
 #pragma unroll
             for (int q = 0; q < PR::kKeep; q++)
-                if (q == s) { g = gr[i][q]; val = vr[i][q]; }
-            if (s >= PR::kKeep) { g = a.idx_in[s * N + vv[i]]; val = vin[s * N + vv[i]]; }
-            // the slot step 1 found, else the one step 2 handed out (its lastpos is set there)
+                if (q == s) { g = L.gr[i][q]; val = L.vr[i][q]; }
+            if (s >= PR::kKeep) { g = a.idx_in[s * N + L.vv[i]]; val = vin[s * N + L.vv[i]]; }
+            // the slot plane_scan found, else the one plane_assign handed out
             int k = 0xFF;
             if constexpr (LoaderSlotCache<R>::value)
                 if (s < PR::kKeep) k = S.pslot[r][s];
@@ -304,6 +329,20 @@ __device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays
     }
     // counts of the next plane, for the next call
     prefetch_counts<TY>(p, a, xp == p.nx - 1 ? 0 : xp + 1, y0, z0, t, cr);
+}
+
+// The three passes with their barriers, for kernels that do not overlap plane_scan with other work.
+template <class R, int KS, int TY>
+__device__ __forceinline__ void load_plane(const StepParams& p, const StepArrays& a, TileSmem<R, KS, TY>& S,
+                                           int rs, int xp, int wpos, int y0, int z0, int t,
+                                           int (&cr)[PlaneRegs<TY>::kPer])
+{
+    PlaneLoad<R, TY> L;
+    plane_scan(p, a, S, xp, wpos, y0, z0, t, cr, L);
+    __syncthreads();
+    plane_assign(S, wpos, t);
+    __syncthreads();
+    plane_fill(p, a, S, rs, xp, y0, z0, t, cr, L);
 }
 
 // Offsets of the q-th Laplacian stencil element (LaplacianStencil::Set order): 27-point stencils
@@ -385,8 +424,18 @@ tile_classify_kernel(const __grid_constant__ StepParams p, const StepArrays a, i
     {
         int xp = x0 - 1 + j;
         xp = xp < 0 ? xp + nx : (xp >= nx ? xp - nx : xp);
-        if (j > 0) __syncthreads();
-        load_plane(p, a, S, j % 3, xp, j - 1, y0, z0, t, cr);
+        // the scan of the incoming plane overlaps the other threads' work on the previous plane;
+        // its barrier also ends that work, and the slot hand-out runs only when a grain is new
+        {
+            PlaneLoad<R, TY> L;
+            const bool added = plane_scan(p, a, S, xp, j - 1, y0, z0, t, cr, L);
+            if (__syncthreads_or(added))
+            {
+                plane_assign(S, j - 1, t);
+                __syncthreads();
+            }
+            plane_fill(p, a, S, j % 3, xp, y0, z0, t, cr, L);
+        }
         __syncthreads();
         if (j < 2 || !inside) continue;
         const int x = x0 + j - 2;
