@@ -71,12 +71,14 @@ __device__ __forceinline__ long long pair_key(int ga, int gb, int G)
     return ga < gb ? (long long)ga * G + gb : (long long)gb * G + ga;
 }
 
-// d F / d dG_b of F(a,b) = allowed*tanh((dG_b - dG_a)/allowed) (or dG_b - dG_a without limiting)
-__device__ __forceinline__ double force_slope(const StepParams& p, const StepArrays& a, int ga, int gb)
+// d F / d dG_b of F(a,b) = allowed*tanh((dG_b - dG_a)/allowed) (or dG_b - dG_a without limiting):
+// 1 - tanh^2, with tanh = F/allowed from the tabulated limited force F (0 where allowed = 0)
+__device__ __forceinline__ double force_slope(const StepParams& p, const StepArrays& a, int ga, int gb, double F)
 {
     if (!p.limiting) return 1.0;
     const double allowed = p.allowed_p[a.gphase[ga] * p.nphases + a.gphase[gb]];
-    const double t = tanh((a.dg[gb] - a.dg[ga]) / allowed);
+    if (allowed == 0.0) return 0.0;
+    const double t = F / allowed;
     return 1.0 - t * t;
 }
 
@@ -142,9 +144,10 @@ __device__ int stages_dual(const StepParams& p, const StepArrays& a, const AdjAr
         for (int i = 0; i < n; i++)
             for (int j = i + 1; j < n; j++)
             {
-                const double slope = force_slope(p, a, g[i], g[j]);
+                const double F = limited_force(p, a, g[i], g[j]);
+                const double slope = force_slope(p, a, g[i], g[j], F);
                 const double dF = aa.tdg ? slope * (aa.tdg[g[j]] - aa.tdg[g[i]]) : 0.0;
-                const Dual locdG = mkd(limited_force(p, a, g[i], g[j]), dF);
+                const Dual locdG = mkd(F, dF);
                 Dual norm = dsqrt(val[i] * val[j]);
                 if (a.gstage[g[i]] == 1 || a.gstage[g[j]] == 1) norm = norm + 1.0e-6;
                 const Dual mob = mkd(pair_mobility(p, a, g[i], g[j]), aa.tmu ? aa.tmu[pair_key(g[i], g[j], G)] : 0.0);
@@ -702,14 +705,19 @@ __device__ __forceinline__ void adjoint_core(const StepParams& p, const StepArra
     for (int i = 0; i < n; i++) lnv[i] = 0.0;
     {
         // the adjoint of each kept field, found by grain in the stored next state (the lists agree
-        // entry by entry when the recomputed step reproduces the stored one)
+        // entry by entry when the recomputed step reproduces the stored one).  Finalize stores the
+        // kept fields in list order, so the k-th kept field is looked up at entry k first and
+        // searched for only when that entry holds another grain.
         const int c1 = aa.cnt1[v];
         double lout[KL];
+        int kept = 0;
         for (int i = 0; i < n; i++)
         {
             lout[i] = 0.0;
             if (!keep[i]) continue;
-            const int s1 = find_entry(aa.cnt1, aa.idx1, N, v, g[i]);
+            int s1 = (kept < c1 && aa.idx1[kept * N + v] == g[i]) ? kept : -1;
+            if (s1 < 0) s1 = find_entry(aa.cnt1, aa.idx1, N, v, g[i]);
+            kept++;
             if (s1 >= 0) lout[i] = aa.lam1[s1 * N + v];
             else st |= kStAdjointMismatch;
         }
@@ -786,7 +794,7 @@ __device__ __forceinline__ void adjoint_core(const StepParams& p, const StepArra
                 const long long key = pair_key(g[i], g[j], G);
                 atomicAdd(&aa.gmu[key], lpv[q] * F * norm * p.pref_df);
                 const double lF = lpv[q] * mob * norm * p.pref_df;
-                const double dFb = lF * force_slope(p, a, g[i], g[j]);
+                const double dFb = lF * force_slope(p, a, g[i], g[j], F);
                 atomicAdd(&aa.gdg[g[j]], dFb);
                 atomicAdd(&aa.gdg[g[i]], -dFb);
                 if (s > 0.0)
