@@ -1111,7 +1111,7 @@ int launch_tlm_step(const StepParams& p, const StepArrays& a, const AdjArrays& a
     return (int)cudaGetLastError();
 }
 
-constexpr int kAdjListBlocks = 148 * 8;   // blocks of each per-length adjoint kernel
+constexpr int kAdjListBlocks = 148 * 32;   // blocks of each per-length adjoint kernel
 
 // The worklist kernel (few voxels, each a long serial chain) runs on the side stream, launched
 // first, so that it overlaps the list-length kernels instead of adding its latency after them.

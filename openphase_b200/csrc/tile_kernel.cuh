@@ -49,7 +49,14 @@ template <class R>
 struct ClassifyVolSlots {
     static constexpr int value = LoaderSlotCache<R>::value ? 128 : 256;
 };
-constexpr int kComputeBlocks = 148 * 8; // blocks of each per-length compute kernel
+// Blocks of each per-length compute kernel: one per 4096 voxels of the grid, between 8 and 32 per
+// SM (a finer split of each length's entries pays on large grids; on small ones the per-block
+// set-up and flush of the grain-volume hash would cost more than it balances).
+inline int compute_blocks(long long n)
+{
+    const long long b = n / 4096;
+    return (int)(b < 148 * 8 ? 148 * 8 : (b > 148 * 32 ? 148 * 32 : b));
+}
 constexpr int kTileTY = kTileRows;   // tile rows (blocks of kTileZ x kTileRows threads)
 
 template <int TY>
@@ -954,13 +961,14 @@ int launch_tiled_ns(const StepParams& p, const StepArrays& a, void* stream, Laun
         if (e != cudaSuccess) return (int)e;
     }
     bucket_scan_kernel<<<kListCap - 1, 1024, 0, s>>>(a, nblocks);
-    list_compute_kernel<R, 2, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
-    list_compute_kernel<R, 3, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
-    list_compute_kernel<R, 4, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
-    list_compute_kernel<R, 5, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
-    list_compute_kernel<R, 6, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
-    list_compute_kernel<R, 7, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
-    list_compute_kernel<R, 8, KS><<<kComputeBlocks, 128, 0, s>>>(p, a, nblocks);
+    const int cb = compute_blocks(p.n);
+    list_compute_kernel<R, 2, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 3, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 4, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 5, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 6, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 7, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
+    list_compute_kernel<R, 8, KS><<<cb, 128, 0, s>>>(p, a, nblocks);
     // general path: one warp per voxel of the worklist
     {
         auto gk = warp_general_kernel<R, KS, KL>;
